@@ -1,0 +1,175 @@
+/*
+ * magasm.h -- C ABI of the B200 (sm_100a) Nedelec element-assembly library.
+ *
+ * This is the drop-in boundary for MagPackage's assembly path. MATLAB reaches
+ * it through the MEX gateways in magpackage_b200/mex/ (same names and
+ * argument lists as the reference's gateways) and a plain C host reaches it
+ * directly (magpackage_b200/harness/replay.c). No torch or CUDA C++ types
+ * appear in the signatures: pointers are plain, streams are passed as void*
+ * (a cudaStream_t, NULL = the legacy default stream).
+ *
+ * Every entry point returns MAG_OK (0) or a negative MAG_E* status and sets a
+ * thread-local message readable with mag_last_error(). Nothing here calls
+ * exit(), traps or asserts on the device; bad inputs are reported, not
+ * dereferenced.
+ *
+ * Index conventions. The MEX-compatible entry points (mag_mex_*) take the
+ * reference's exact layout: MATLAB column-major doubles, 1-based node/dof ids
+ * stored as doubles, Signs as +-1 doubles. The handle-based entry points take
+ * int32 0-based arrays in device memory: T [Ne][4], dofs [Ne][6] (-1 = no dof,
+ * the reference's dof 0), tags [Ne] (1-based material tags as in RegionTags).
+ * Row-major [Ne][k] equals MATLAB's [k x Ne] column-major, so the same buffer
+ * serves both.
+ */
+#ifndef MAGASM_H
+#define MAGASM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MAG_OK 0
+#define MAG_E_ARG (-1)       /* bad argument (null pointer, size, count) */
+#define MAG_E_RANGE (-2)     /* index out of range (node, dof, tag) */
+#define MAG_E_GEOMETRY (-3)  /* degenerate element (det == 0 or not finite) */
+#define MAG_E_CUDA (-4)      /* CUDA runtime error */
+#define MAG_E_TIMEOUT (-5)   /* a bounded device-side wait gave up */
+#define MAG_E_NOMEM (-6)     /* device allocation failed */
+#define MAG_E_UNSUPPORTED (-7)
+
+typedef struct mag_mesh mag_mesh; /* opaque, device-resident mesh + CSR plan */
+
+typedef struct {
+    int64_t num_nodes;
+    int64_t num_elements;
+    int64_t num_dofs;       /* CSR rows/cols */
+    int64_t nnz;            /* structural nonzeros (union of element couplings) */
+    int64_t num_incidences; /* (element, local edge) pairs with a dof */
+    int32_t max_row_nnz;
+    int32_t wide_positions; /* 1 if some row exceeds 31 entries */
+    int32_t signs_derived;  /* 1 if signs equal the Mesh.m:134 rule and are not stored */
+    int32_t reserved;
+    int64_t device_bytes;   /* memory held by the handle */
+} mag_mesh_info;
+
+/* ---- library ------------------------------------------------------------ */
+
+int mag_version(void);
+const char *mag_last_error(void);
+
+/* ---- topology ------------------------------------------------------------ */
+
+/* Mesh.generateEdges (src/Mesh.m:114-138) on the GPU. d_T: int32 [Ne][4],
+ * 0-based nodes. Outputs (device): d_edges [E][2] 0-based (lexicographic by
+ * (min,max) node; capacity 6*Ne rows), d_t2e [Ne][6] 0-based edge ids,
+ * d_sign [Ne][6] (+1 iff the local start node has the smaller id). *E_out is
+ * written on the host after the call completes (the call synchronises). */
+int mag_generate_edges(const int32_t *d_T, int64_t Ne, int64_t Nn, int32_t *d_edges,
+                       int32_t *d_t2e, int8_t *d_sign, int64_t *E_out, void *stream);
+
+/* ---- mesh handle: one-time CSR plan -------------------------------------- */
+
+/* Copies the mesh into the handle's layout and builds, on the GPU, the CSR
+ * pattern of the dof-dof coupling (rows/cols = dofs, columns sorted) and the
+ * per-row incidence list (element, local edge, position of each of its six
+ * couplings inside the row) that the assembly's fixed-order reduction uses.
+ * This is the reference's unique()/sparse() structure work (Mesh.m:126-135,
+ * Assembler.m:37-38) done once per mesh. d_signs may be NULL (derive from T,
+ * the Mesh.m:134-135 rule); when given and equal to that rule it is not stored.
+ * All inputs are device pointers; the handle keeps its own copies. */
+int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t Ne,
+                    const int32_t *d_dofs, const int8_t *d_signs, const int32_t *d_tags,
+                    int64_t num_dofs, mag_mesh **out, void *stream);
+int mag_mesh_destroy(mag_mesh *mesh);
+int mag_mesh_get_info(const mag_mesh *mesh, mag_mesh_info *info);
+/* Copy the structural pattern out (device buffers: row_ptr [num_dofs+1], col_idx [nnz]). */
+int mag_mesh_pattern(const mag_mesh *mesh, int64_t *d_row_ptr, int32_t *d_col_idx, void *stream);
+
+/* Quadrature and reference basis, exactly what Assembler.m passes to the MEX
+ * (Assembler.m:30-32,191-193): Qw [nq], CurlRef and ValRef [6 x 3 x nq]
+ * column-major (entry (i,c,q) at i + 6c + 18q). Host pointers; nq <= 16. */
+int mag_mesh_set_quadrature(mag_mesh *mesh, const double *qw, int nq, const double *curl_ref,
+                            const double *val_ref);
+
+/* Material tables in the layout of Assembler.packMaterialData
+ * (src/Assembler.m:270-304): eight host arrays indexed by tag-1, nmat entries
+ * each, breaks/coefs concatenated. Consumed by MexMaterialUtils.hpp:24-87's
+ * rule (binary search, Horner, linear extrapolation past maxB, clamps). */
+int mag_mesh_set_materials(mag_mesh *mesh, const double *lin_nu, const double *is_nonlinear,
+                           const double *max_bsq, int nmat, const double *breaks, int nbreaks,
+                           const double *coefs, int ncoefs, const double *spline_start,
+                           const double *spline_count, const double *coef_start);
+
+/* ---- assembly into the structural CSR (device buffers) -------------------- */
+
+/* Newton Jacobian values and residual: the work of
+ * assemble_jacobian_kernel_mex.cpp:61-152 followed by the sparse() sums of
+ * Assembler.m:205-206,214-215, fused. d_sol [num_dofs] is SolA; d_vals [nnz]
+ * receives J (ignored when calc_j == 0, like CalcJ = false); d_res [num_dofs]
+ * receives the residual. Values are summed per nonzero in ascending element
+ * order by a fixed-order reduction: deterministic, no floating-point atomics. */
+int mag_assemble_jacobian(mag_mesh *mesh, const double *d_sol, double *d_vals, double *d_res,
+                          int calc_j, void *stream);
+
+/* Curl-curl stiffness K(nu) with a per-element reluctivity d_nu [Ne]
+ * (assemble_curl_curl_kernel_mex.cpp:18-121 + Assembler.m:37-38). */
+int mag_assemble_stiffness(mag_mesh *mesh, const double *d_nu, double *d_vals, void *stream);
+
+/* Sigma-weighted Nedelec mass M(sigma) (assemble_mass_kernel_mex.cpp:17-127 +
+ * Assembler.m:52-53,71-72). d_sigma [Ne], or NULL for sigma = 1 (the
+ * reference's empty Coeffs, assemble_mass_kernel_mex.cpp:155,187). */
+int mag_assemble_mass(mag_mesh *mesh, const double *d_sigma, double *d_vals, void *stream);
+
+/* Source vector F (assemble_source_kernel_mex.cpp:16-114 + Assembler.m:87-89).
+ * d_js [Ne][3] current density per element; d_out [num_dofs]. */
+int mag_assemble_source(mag_mesh *mesh, const double *d_js, double *d_out, void *stream);
+
+/* Element magnetic flux density B [Ne][3] and |B|^2 [Ne] at the solution
+ * d_sol (the per-element curl of PostProcessor.computeElementB,
+ * src/post/PostProcessor.m:64-126, evaluated as the Jacobian kernel does). */
+int mag_element_b(mag_mesh *mesh, const double *d_sol, double *d_b, double *d_bsq, void *stream);
+
+/* MATLAB sparse() storage: drop entries whose value is exactly zero (MATLAB
+ * keeps no explicit zeros). Inputs: a CSR over nrows rows. Outputs must hold
+ * nrows+1 / nnz entries; *nnz_out is written on the host (the call synchronises).
+ * d_vals_out may alias nothing of the inputs. */
+int mag_csr_drop_zeros(const int64_t *d_row_ptr, const int32_t *d_col_idx, const double *d_vals,
+                       int64_t nrows, int64_t *d_row_ptr_out, int32_t *d_col_out,
+                       double *d_vals_out, int64_t *nnz_out, void *stream);
+
+/* ---- MEX-compatible entry points (host buffers, reference layout) --------- */
+
+/* [I,J,V,R_idx,R_val] = assemble_jacobian_kernel_mex(P,T,Dofs,Signs,Tags,SolA,
+ *   Qw,CurlRef,lin,isNon,maxB,brk,coe,start,cnt,coeStart,calcJ)
+ * (src/mex/assemble_jacobian_kernel_mex.cpp:8-153, 17 inputs). All arrays are
+ * host doubles in MATLAB layout; outputs are host buffers sized 36*Ne (I,J,V;
+ * untouched when calc_j == 0) and 6*Ne (R_idx, R_val), triplets in the
+ * reference's order (element-major, local column j outer, row i inner). */
+int mag_mex_jacobian(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                     const double *Signs, const double *Tags, const double *SolA, int64_t Ndof,
+                     const double *Qw, int nq, const double *CurlRef, const double *lin,
+                     const double *isNon, const double *maxB, int nmat, const double *brk,
+                     int nbrk, const double *coe, int ncoe, const double *start,
+                     const double *cnt, const double *coeStart, int calc_j, double *I,
+                     double *J, double *V, double *R_idx, double *R_val);
+
+/* [I,J,V] = assemble_curl_curl_kernel_mex(P,T,Dofs,Signs,Nu,Qw,CurlRef)
+ * (src/mex/assemble_curl_curl_kernel_mex.cpp:18-121). */
+int mag_mex_curl_curl(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                      const double *Signs, const double *Nu, const double *Qw, int nq,
+                      const double *CurlRef, double *I, double *J, double *V);
+
+/* [I,J,V] = assemble_mass_kernel_mex(P,T,Dofs,Signs,Coeffs,Qw,ValRef)
+ * (src/mex/assemble_mass_kernel_mex.cpp:17-127). ncoeffs != Ne means sigma = 1. */
+int mag_mex_mass(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                 const double *Signs, const double *Coeffs, int64_t ncoeffs, const double *Qw,
+                 int nq, const double *ValRef, double *I, double *J, double *V);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAGASM_H */

@@ -1,0 +1,598 @@
+// Element assembly kernels (FP64, sm_100a).
+//
+// Two phases per assembly:
+//   phase 1 (element-parallel): each element's 6x6 block (with edge signs
+//     applied) and its 6 residual/RHS entries go to a scratch slab laid out
+//     [element][local row][8] = {row values 0..5, vector entry, pad}: one
+//     64-byte aligned chunk per (element, local row).
+//   phase 2 (row-parallel): every CSR row walks its incidence list, which the
+//     pattern builder sorted by ascending element, and adds each incident
+//     element's chunk into the row's slots. Every nonzero is therefore summed
+//     in one fixed order (element order, the order of appearance that MATLAB's
+//     sparse() sees in the MEX triplets), with no floating-point atomics.
+//
+// Bit-exactness. This translation unit is compiled with -fmad=false and the
+// element arithmetic follows the reference's evaluation order
+// (src/mex/assemble_jacobian_kernel_mex.cpp:61-152, MexElemUtils.hpp:35-66,
+// MexMaterialUtils.hpp:24-87, assemble_curl_curl_kernel_mex.cpp:44-121,
+// assemble_mass_kernel_mex.cpp:167-248, assemble_source_kernel_mex.cpp:46-114),
+// so each element block equals the reference MEX output bit for bit. Where the
+// reference repeats identical work per quadrature point (the Nedelec curl is
+// constant), the value is computed once and the per-point products are
+// accumulated in the reference's order, which yields the same bits.
+#include "assemble.cuh"
+#include "common.cuh"
+
+namespace mag {
+
+namespace {
+
+__device__ __forceinline__ unsigned derived_signs(int4 t) {
+    // bit k set <=> local edge k runs from the larger to the smaller node id
+    int n[4] = {t.x, t.y, t.z, t.w};
+    unsigned b = 0;
+#pragma unroll
+    for (int k = 0; k < 6; k++) b |= (n[edge_a(k)] < n[edge_b(k)] ? 0u : 1u) << k;
+    return b;
+}
+
+__device__ __forceinline__ double flip(double v, unsigned neg) { return neg ? -v : v; }
+
+struct Geo {
+    double J[3][3];
+    double det, rdet, adet;
+};
+
+__device__ __forceinline__ void geometry(const double4 *__restrict__ xyz, int4 t, Geo &g) {
+    double4 v0 = xyz[t.x], v1 = xyz[t.y], v2 = xyz[t.z], v3 = xyz[t.w];
+    g.J[0][0] = v1.x - v0.x; g.J[1][0] = v1.y - v0.y; g.J[2][0] = v1.z - v0.z;
+    g.J[0][1] = v2.x - v0.x; g.J[1][1] = v2.y - v0.y; g.J[2][1] = v2.z - v0.z;
+    g.J[0][2] = v3.x - v0.x; g.J[1][2] = v3.y - v0.y; g.J[2][2] = v3.z - v0.z;
+    const double(*J)[3] = g.J;
+    double m0 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    double m1 = J[1][0] * J[2][2] - J[1][2] * J[2][0];
+    double m2 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    g.det = J[0][0] * m0 - J[0][1] * m1 + J[0][2] * m2;
+    g.rdet = 1.0 / g.det;
+    g.adet = fabs(g.det);
+}
+
+// Physical curls of the six Whitney functions, C_i = J c_i / det, for the
+// standard reference curls c = 2 grad(L_a) x grad(L_b):
+//   (0,-2,2) (2,0,-2) (-2,2,0) (0,0,2) (0,-2,0) (2,0,0).
+// The reference forms J c with three products and two additions; with these
+// c entries that sum is exactly 2(J_b - J_a) (scaling by 2 and adding signed
+// zeros are exact), and 2 d / det rounds like d * (2/det).
+__device__ __forceinline__ void curls_standard(const Geo &g, double C[6][3]) {
+    double r2 = 2.0 * g.rdet;
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        C[0][r] = (g.J[r][2] - g.J[r][1]) * r2;
+        C[1][r] = (g.J[r][0] - g.J[r][2]) * r2;
+        C[2][r] = (g.J[r][1] - g.J[r][0]) * r2;
+        C[3][r] = g.J[r][2] * r2;
+        C[4][r] = -(g.J[r][1] * r2);
+        C[5][r] = g.J[r][0] * r2;
+    }
+}
+
+// Any reference curl table (entry (i,c) of point q at i + 6c + 18q).
+__device__ __forceinline__ void curls_generic(const Geo &g, const double *__restrict__ ref, int q,
+                                              double C[6][3]) {
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        double c0 = ref[i + 18 * q], c1 = ref[i + 6 + 18 * q], c2 = ref[i + 12 + 18 * q];
+#pragma unroll
+        for (int r = 0; r < 3; r++) C[i][r] = (g.J[r][0] * c0 + g.J[r][1] * c1 + g.J[r][2] * c2) * g.rdet;
+    }
+}
+
+__device__ __forceinline__ double dot3(const double *a, const double *b) {
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+// nu(s) and d nu/ds, s = |B|^2, per MexMaterialUtils.hpp:24-87.
+__device__ __forceinline__ void material_eval(const MaterialParams &mp, int tag, double s,
+                                              double &nu, double &dnu) {
+    int m = tag - 1;
+    if (__ldg(mp.is_non + m) == 0.0) {
+        nu = __ldg(mp.lin + m);
+        dnu = 0.0;
+        return;
+    }
+    double smax = __ldg(mp.max_bsq + m);
+    bool beyond = s > smax;
+    double x = beyond ? smax : s;
+    const double *b = mp.breaks + __ldg(mp.start + m);
+    int pieces = __ldg(mp.count + m);
+    int k = 0, lo = 0, hi = pieces - 1;
+    while (lo <= hi) {
+        int mid = lo + (hi - lo) / 2;
+        if (x >= __ldg(b + mid)) {
+            k = mid;
+            lo = mid + 1;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    if (k >= pieces) k = pieces - 1;
+    if (k < 0) k = 0;
+    const double *c = mp.coefs + __ldg(mp.coef_start + m) + 4 * k;
+    double c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2), c3 = __ldg(c + 3);
+    double t = x - __ldg(b + k);
+    double v = ((c0 * t + c1) * t + c2) * t + c3;
+    double dv = (3.0 * c0 * t + 2.0 * c1) * t + c2;
+    if (beyond) v = v + dv * (s - smax);
+    double nu0 = __ldg(mp.lin + m);
+    if (v > nu0 || v < 1e-7) {
+        v = nu0;
+        dv = 0.0;
+    }
+    nu = v;
+    dnu = dv;
+}
+
+__device__ __forceinline__ void load_dofs(const int32_t *__restrict__ dofs, int64_t e, int d[6]) {
+    const int2 *p = reinterpret_cast<const int2 *>(dofs + 6 * e);
+    int2 a = p[0], b = p[1], c = p[2];
+    d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y; d[4] = c.x; d[5] = c.y;
+}
+
+// Sum over quadrature points of v * w_q, accumulated in point order from zero.
+__device__ __forceinline__ double qsum(double v, const double *w, int nq, int uniform) {
+    double u = v * w[0];
+    double acc = u;
+    if (uniform) {
+        for (int q = 1; q < nq; q++) acc = acc + u;
+    } else {
+        for (int q = 1; q < nq; q++) acc = acc + v * w[q];
+    }
+    return acc;
+}
+
+__device__ __forceinline__ void store_row(double *__restrict__ dst, const double k[6], double r) {
+    double2 *p = reinterpret_cast<double2 *>(dst);
+    p[0] = make_double2(k[0], k[1]);
+    p[1] = make_double2(k[2], k[3]);
+    p[2] = make_double2(k[4], k[5]);
+    p[3] = make_double2(r, 0.0);
+}
+
+// ---- phase 1: Jacobian + residual -------------------------------------------
+
+template <bool CALCJ, bool STDCURL>
+__global__ void __launch_bounds__(128) k_jacobian_elems(ElemData m, const double *__restrict__ sol,
+                                                        QuadParams qp, MaterialParams mp,
+                                                        double *__restrict__ scratch) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    int4 t = m.tet[e];
+    int d[6];
+    load_dofs(m.dofs, e, d);
+    unsigned sb = m.signbits ? m.signbits[e] : derived_signs(t);
+    int tag = m.tags[e];
+    Geo g;
+    geometry(m.xyz, t, g);
+    double a[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) a[i] = d[i] >= 0 ? flip(__ldg(sol + d[i]), (sb >> i) & 1) : 0.0;
+    double w[kMaxQuad];
+    for (int q = 0; q < qp.nq; q++) w[q] = qp.qw[q] * g.adet;
+
+    double res[6], K[6][6];
+    if (STDCURL) {
+        double C[6][3];
+        curls_standard(g, C);
+        double B[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double s = a[0] * C[0][c];
+#pragma unroll
+            for (int i = 1; i < 6; i++) s = s + a[i] * C[i][c];
+            B[c] = s;
+        }
+        double nu, dnu;
+        material_eval(mp, tag, dot3(B, B), nu, dnu);
+        double b[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            b[i] = dot3(B, C[i]);
+            res[i] = qsum(nu * b[i], w, qp.nq, qp.uniform_w);
+        }
+        if (CALCJ) {
+            if (dnu == 0.0) {
+                // linear response: nu*Ci.Cj + (+-0) is symmetric bit for bit
+#pragma unroll
+                for (int i = 0; i < 6; i++)
+#pragma unroll
+                    for (int j = i; j < 6; j++) {
+                        double v = qsum(nu * dot3(C[i], C[j]), w, qp.nq, qp.uniform_w);
+                        K[i][j] = v;
+                        K[j][i] = v;
+                    }
+            } else {
+                double g2 = 2.0 * dnu;
+#pragma unroll
+                for (int i = 0; i < 6; i++) {
+                    double gi = g2 * b[i];
+#pragma unroll
+                    for (int j = 0; j < 6; j++)
+                        K[i][j] = qsum(nu * dot3(C[i], C[j]) + gi * b[j], w, qp.nq, qp.uniform_w);
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            res[i] = 0.0;
+#pragma unroll
+            for (int j = 0; j < 6; j++) K[i][j] = 0.0;
+        }
+        for (int q = 0; q < qp.nq; q++) {
+            double C[6][3];
+            curls_generic(g, qp.curl_ref, q, C);
+            double B[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int i = 0; i < 6; i++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) B[c] = B[c] + a[i] * C[i][c];
+            double nu, dnu;
+            material_eval(mp, tag, dot3(B, B), nu, dnu);
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                double bi = dot3(B, C[i]);
+                res[i] = res[i] + nu * bi * w[q];
+                if (CALCJ) {
+#pragma unroll
+                    for (int j = 0; j < 6; j++)
+                        K[i][j] = K[i][j] + (nu * dot3(C[i], C[j]) + 2.0 * dnu * bi * dot3(B, C[j])) * w[q];
+                }
+            }
+        }
+    }
+    double *dst = scratch + e * kScratchPerElem;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        double row[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) row[j] = CALCJ ? flip(K[i][j], ((sb >> i) ^ (sb >> j)) & 1) : 0.0;
+        store_row(dst + i * kScratchStride, row, flip(res[i], (sb >> i) & 1));
+    }
+}
+
+// ---- phase 1: curl-curl K(nu) ----------------------------------------------
+
+template <bool STDCURL>
+__global__ void __launch_bounds__(128) k_stiffness_elems(ElemData m, const double *__restrict__ nu_e,
+                                                         QuadParams qp, double *__restrict__ scratch) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    int4 t = m.tet[e];
+    unsigned sb = m.signbits ? m.signbits[e] : derived_signs(t);
+    Geo g;
+    geometry(m.xyz, t, g);
+    double nu = nu_e[e];
+    double w[kMaxQuad];
+    for (int q = 0; q < qp.nq; q++) w[q] = qp.qw[q] * g.adet;
+    double K[6][6];
+    if (STDCURL) {
+        double C[6][3];
+        curls_standard(g, C);
+#pragma unroll
+        for (int i = 0; i < 6; i++)
+#pragma unroll
+            for (int j = i; j < 6; j++) {
+                double v = qsum(dot3(C[i], C[j]) * nu, w, qp.nq, qp.uniform_w);
+                K[i][j] = v;
+                K[j][i] = v;
+            }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 6; i++)
+#pragma unroll
+            for (int j = 0; j < 6; j++) K[i][j] = 0.0;
+        for (int q = 0; q < qp.nq; q++) {
+            double C[6][3];
+            curls_generic(g, qp.curl_ref, q, C);
+#pragma unroll
+            for (int i = 0; i < 6; i++)
+#pragma unroll
+                for (int j = 0; j < 6; j++) K[i][j] = K[i][j] + dot3(C[i], C[j]) * nu * w[q];
+        }
+    }
+    double *dst = scratch + e * kScratchPerElem;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        double row[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) row[j] = flip(K[i][j], ((sb >> i) ^ (sb >> j)) & 1);
+        store_row(dst + i * kScratchStride, row, 0.0);
+    }
+}
+
+// ---- phase 1: sigma-mass M(sigma) and source F ---------------------------------
+
+__device__ __forceinline__ void inverse3(const Geo &g, double iv[3][3]) {
+    const double(*J)[3] = g.J;
+    double s = 1.0 / g.det;
+    iv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) * s;
+    iv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * s;
+    iv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * s;
+    iv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) * s;
+    iv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * s;
+    iv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * s;
+    iv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) * s;
+    iv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * s;
+    iv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * s;
+}
+
+__global__ void __launch_bounds__(128) k_mass_elems(ElemData m, const double *__restrict__ sigma_e,
+                                                    QuadParams qp, double *__restrict__ scratch) {
+    __shared__ double sref[18 * kMaxQuad];
+    for (int i = threadIdx.x; i < 18 * qp.nq; i += blockDim.x) sref[i] = qp.val_ref[i];
+    __syncthreads();
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    int4 t = m.tet[e];
+    unsigned sb = m.signbits ? m.signbits[e] : derived_signs(t);
+    Geo g;
+    geometry(m.xyz, t, g);
+    double iv[3][3];
+    inverse3(g, iv);
+    double sigma = sigma_e ? sigma_e[e] : 1.0;
+    double M[6][6];
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int j = 0; j < 6; j++) M[i][j] = 0.0;
+    if (fabs(sigma) > 1e-12) {  // zero-sigma elements contribute explicit zeros
+        for (int q = 0; q < qp.nq; q++) {
+            double w = qp.qw[q] * g.adet;
+            double N[6][3];
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                double r0 = sref[i + 18 * q], r1 = sref[i + 6 + 18 * q], r2 = sref[i + 12 + 18 * q];
+#pragma unroll
+                for (int c = 0; c < 3; c++) N[i][c] = iv[0][c] * r0 + iv[1][c] * r1 + iv[2][c] * r2;
+            }
+#pragma unroll
+            for (int i = 0; i < 6; i++)
+#pragma unroll
+                for (int j = i; j < 6; j++) {
+                    double v = M[i][j] + dot3(N[i], N[j]) * sigma * w;
+                    M[i][j] = v;
+                    M[j][i] = v;
+                }
+        }
+    }
+    double *dst = scratch + e * kScratchPerElem;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        double row[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) row[j] = flip(M[i][j], ((sb >> i) ^ (sb >> j)) & 1);
+        store_row(dst + i * kScratchStride, row, 0.0);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_source_elems(ElemData m, const double *__restrict__ js,
+                                                      QuadParams qp, double *__restrict__ scratch) {
+    __shared__ double sref[18 * kMaxQuad];
+    for (int i = threadIdx.x; i < 18 * qp.nq; i += blockDim.x) sref[i] = qp.val_ref[i];
+    __syncthreads();
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    int4 t = m.tet[e];
+    unsigned sb = m.signbits ? m.signbits[e] : derived_signs(t);
+    Geo g;
+    geometry(m.xyz, t, g);
+    double iv[3][3];
+    inverse3(g, iv);
+    double jp[3] = {js[3 * e], js[3 * e + 1], js[3 * e + 2]};
+    double jr[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) jr[r] = iv[r][0] * jp[0] + iv[r][1] * jp[1] + iv[r][2] * jp[2];
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    if (fabs(jp[0]) > 1e-12 || fabs(jp[1]) > 1e-12 || fabs(jp[2]) > 1e-12) {
+        for (int q = 0; q < qp.nq; q++) {
+            double w = qp.qw[q] * g.adet;
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                double r[3] = {sref[i + 18 * q], sref[i + 6 + 18 * q], sref[i + 12 + 18 * q]};
+                f[i] = f[i] + dot3(jr, r) * w;
+            }
+        }
+    }
+    double *dst = scratch + e * kScratchPerElem;
+#pragma unroll
+    for (int i = 0; i < 6; i++) dst[i * kScratchStride + 6] = flip(f[i], (sb >> i) & 1);
+}
+
+// ---- element B (post-processing / predictor features) -------------------------
+
+__global__ void __launch_bounds__(128) k_element_b(ElemData m, const double *__restrict__ sol,
+                                                   double *__restrict__ bout, double *__restrict__ bsq) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    int4 t = m.tet[e];
+    int d[6];
+    load_dofs(m.dofs, e, d);
+    unsigned sb = m.signbits ? m.signbits[e] : derived_signs(t);
+    Geo g;
+    geometry(m.xyz, t, g);
+    double C[6][3];
+    curls_standard(g, C);
+    double a[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) a[i] = d[i] >= 0 ? flip(__ldg(sol + d[i]), (sb >> i) & 1) : 0.0;
+    double B[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        double s = a[0] * C[0][c];
+#pragma unroll
+        for (int i = 1; i < 6; i++) s = s + a[i] * C[i][c];
+        B[c] = s;
+    }
+    if (bout) {
+        bout[3 * e] = B[0];
+        bout[3 * e + 1] = B[1];
+        bout[3 * e + 2] = B[2];
+    }
+    if (bsq) bsq[e] = dot3(B, B);
+}
+
+// ---- phase 2: fixed-order row reduction --------------------------------------
+
+template <bool MAT, bool VEC, bool WIDE>
+__global__ void __launch_bounds__(128) k_rows_reduce(RowPlan rp, const double *__restrict__ scratch,
+                                                     double *__restrict__ vals, double *__restrict__ vec) {
+    extern __shared__ double sacc[];
+    int64_t a0 = (int64_t)blockIdx.x * blockDim.x;
+    int64_t a = a0 + threadIdx.x;
+    int64_t a_end = a0 + blockDim.x < rp.ndof ? a0 + blockDim.x : rp.ndof;
+    int32_t base = rp.row_ptr[a0];
+    int32_t span = rp.row_ptr[a_end] - base;
+    if (MAT) {
+        for (int32_t i = threadIdx.x; i < span; i += blockDim.x) sacc[i] = 0.0;
+        __syncthreads();
+    }
+    if (a < rp.ndof) {
+        int32_t off = MAT ? rp.row_ptr[a] - base : 0;
+        double r = 0.0;
+        int32_t t1 = rp.inc_ptr[a + 1];
+        for (int32_t t = rp.inc_ptr[a]; t < t1; t++) {
+            uint32_t ew = rp.inc_elem[t];
+            const double *src = scratch + (int64_t)(ew & 0x1FFFFFFFu) * kScratchPerElem +
+                                (ew >> 29) * kScratchStride;
+            if (MAT) {
+                const double2 *p2 = reinterpret_cast<const double2 *>(src);
+                double2 v01 = __ldg(p2), v23 = __ldg(p2 + 1), v45 = __ldg(p2 + 2);
+                double v[6] = {v01.x, v01.y, v23.x, v23.y, v45.x, v45.y};
+                if (!WIDE) {
+                    uint32_t pw = rp.inc_pos[t];
+#pragma unroll
+                    for (int j = 0; j < 6; j++) {
+                        uint32_t p = (pw >> (5 * j)) & 31u;
+                        if (p != (uint32_t)kCompactMaxRow) sacc[off + p] = sacc[off + p] + v[j];
+                    }
+                } else {
+                    uint32_t w0 = rp.inc_pos[2 * (int64_t)t], w1 = rp.inc_pos[2 * (int64_t)t + 1];
+#pragma unroll
+                    for (int j = 0; j < 6; j++) {
+                        uint32_t p = (j < 4 ? (w0 >> (8 * j)) : (w1 >> (8 * (j - 4)))) & 255u;
+                        if (p != (uint32_t)kWideMaxRow) sacc[off + p] = sacc[off + p] + v[j];
+                    }
+                }
+            }
+            if (VEC) r = r + __ldg(src + 6);
+        }
+        if (VEC) vec[a] = r;
+    }
+    if (MAT) {
+        __syncthreads();
+        for (int32_t i = threadIdx.x; i < span; i += blockDim.x) vals[base + i] = sacc[i];
+    }
+}
+
+// ---- MEX layout -------------------------------------------------------------
+
+// Scratch -> reference triplets: entry (i, j) of element e at 36e + 6j + i.
+__global__ void k_to_triplets(const double *__restrict__ scratch, const int32_t *__restrict__ dofs,
+                              int64_t ne, int calcj, double *__restrict__ I, double *__restrict__ J,
+                              double *__restrict__ V, double *__restrict__ Ridx,
+                              double *__restrict__ Rval) {
+    int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= 36 * ne) return;
+    int64_t e = s / 36;
+    int r = (int)(s - 36 * e);
+    int j = r / 6, i = r - 6 * j;
+    const double *src = scratch + e * kScratchPerElem;
+    if (calcj) {
+        I[s] = (double)(dofs[6 * e + i] + 1);
+        J[s] = (double)(dofs[6 * e + j] + 1);
+        V[s] = src[i * kScratchStride + j];
+    }
+    if (Ridx && r < 6) {
+        Ridx[6 * e + r] = (double)(dofs[6 * e + r] + 1);
+        Rval[6 * e + r] = src[r * kScratchStride + 6];
+    }
+}
+
+inline unsigned blocks(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+// ---- launchers -----------------------------------------------------------------
+
+int launch_jacobian_elems(const ElemData &m, const double *sol, const QuadParams &qp,
+                          const MaterialParams &mp, int calcj, double *scratch, cudaStream_t s) {
+    unsigned g = blocks(m.ne, 128);
+    if (qp.standard_curl) {
+        if (calcj) k_jacobian_elems<true, true><<<g, 128, 0, s>>>(m, sol, qp, mp, scratch);
+        else k_jacobian_elems<false, true><<<g, 128, 0, s>>>(m, sol, qp, mp, scratch);
+    } else {
+        if (calcj) k_jacobian_elems<true, false><<<g, 128, 0, s>>>(m, sol, qp, mp, scratch);
+        else k_jacobian_elems<false, false><<<g, 128, 0, s>>>(m, sol, qp, mp, scratch);
+    }
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+int launch_stiffness_elems(const ElemData &m, const double *nu, const QuadParams &qp,
+                           double *scratch, cudaStream_t s) {
+    unsigned g = blocks(m.ne, 128);
+    if (qp.standard_curl) k_stiffness_elems<true><<<g, 128, 0, s>>>(m, nu, qp, scratch);
+    else k_stiffness_elems<false><<<g, 128, 0, s>>>(m, nu, qp, scratch);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+int launch_mass_elems(const ElemData &m, const double *sigma, const QuadParams &qp, double *scratch,
+                      cudaStream_t s) {
+    k_mass_elems<<<blocks(m.ne, 128), 128, 0, s>>>(m, sigma, qp, scratch);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+int launch_source_elems(const ElemData &m, const double *js, const QuadParams &qp, double *scratch,
+                        cudaStream_t s) {
+    k_source_elems<<<blocks(m.ne, 128), 128, 0, s>>>(m, js, qp, scratch);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+int launch_element_b(const ElemData &m, const double *sol, double *b, double *bsq, cudaStream_t s) {
+    k_element_b<<<blocks(m.ne, 128), 128, 0, s>>>(m, sol, b, bsq);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+int launch_rows_reduce(const RowPlan &rp, int max_row, const double *scratch, double *vals,
+                       double *vec, cudaStream_t s) {
+    const int b = 128;
+    unsigned g = blocks(rp.ndof, b);
+    size_t smem = vals ? (size_t)b * max_row * sizeof(double) : 0;
+    if (smem > 200 * 1024) return MAG_E_UNSUPPORTED;
+    bool mat = vals != nullptr, v = vec != nullptr;
+#define MAG_P2(M, V, W)                                                                          \
+    do {                                                                                         \
+        auto kern = k_rows_reduce<M, V, W>;                                                      \
+        if (smem > 48 * 1024)                                                                    \
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+        kern<<<g, b, smem, s>>>(rp, scratch, vals, vec);                                         \
+    } while (0)
+    if (rp.wide) {
+        if (mat && v) MAG_P2(true, true, true);
+        else if (mat) MAG_P2(true, false, true);
+        else if (v) MAG_P2(false, true, true);
+    } else {
+        if (mat && v) MAG_P2(true, true, false);
+        else if (mat) MAG_P2(true, false, false);
+        else if (v) MAG_P2(false, true, false);
+    }
+#undef MAG_P2
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+int launch_to_triplets(const double *scratch, const int32_t *dofs, int64_t ne, int calcj, double *I,
+                       double *J, double *V, double *Ridx, double *Rval, cudaStream_t s) {
+    k_to_triplets<<<blocks(36 * ne, 256), 256, 0, s>>>(scratch, dofs, ne, calcj, I, J, V, Ridx, Rval);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+}  // namespace mag

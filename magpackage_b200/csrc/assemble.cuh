@@ -1,0 +1,24 @@
+// Launchers for the assembly kernels (defined in assemble.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace mag {
+
+int launch_jacobian_elems(const ElemData &m, const double *sol, const QuadParams &qp,
+                          const MaterialParams &mp, int calcj, double *scratch, cudaStream_t s);
+int launch_stiffness_elems(const ElemData &m, const double *nu, const QuadParams &qp,
+                           double *scratch, cudaStream_t s);
+int launch_mass_elems(const ElemData &m, const double *sigma, const QuadParams &qp, double *scratch,
+                      cudaStream_t s);
+int launch_source_elems(const ElemData &m, const double *js, const QuadParams &qp, double *scratch,
+                        cudaStream_t s);
+int launch_element_b(const ElemData &m, const double *sol, double *b, double *bsq, cudaStream_t s);
+int launch_rows_reduce(const RowPlan &rp, int max_row, const double *scratch, double *vals,
+                       double *vec, cudaStream_t s);
+int launch_to_triplets(const double *scratch, const int32_t *dofs, int64_t ne, int calcj, double *I,
+                       double *J, double *V, double *Ridx, double *Rval, cudaStream_t s);
+
+}  // namespace mag

@@ -1,0 +1,755 @@
+// C ABI (include/magasm.h): the mesh handle, validation, and the
+// MEX-compatible entry points.
+#include <cstdarg>
+#include <cstring>
+#include <new>
+
+#include "assemble.cuh"
+#include "common.cuh"
+#include "internal.h"
+
+namespace mag {
+
+namespace {
+thread_local char g_err[768] = "";
+}
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+namespace {
+
+constexpr int kB = 256;
+inline unsigned grid(int64_t n) { return (unsigned)((n + kB - 1) / kB); }
+
+// ---- input conversion / validation kernels ---------------------------------
+
+__global__ void k_pack_xyz(const double *__restrict__ P, int64_t nn, double4 *__restrict__ xyz,
+                           int *__restrict__ err) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    double x = P[3 * i], y = P[3 * i + 1], z = P[3 * i + 2];
+    if (!isfinite(x) || !isfinite(y) || !isfinite(z)) atomicExch(err, 1);
+    xyz[i] = make_double4(x, y, z, 0.0);
+}
+
+// 1-based node ids stored as doubles (MEX layout) -> 0-based int32.
+__global__ void k_index_from_double(const double *__restrict__ src, int64_t n, int32_t *__restrict__ dst,
+                                    int64_t limit, int allow_zero, int *__restrict__ err) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = src[i];
+    // the reference truncates with (int) before use
+    int64_t k = (v > -2.0 && v < 4294967296.0) ? (int64_t)v : -2;
+    if (k < (allow_zero ? 0 : 1) || k > limit) {
+        atomicExch(err, 1);
+        k = allow_zero ? 0 : 1;
+    }
+    dst[i] = (int32_t)(k - 1);
+}
+
+__global__ void k_check_nodes(const int4 *__restrict__ tet, int64_t ne, int64_t nn, int *__restrict__ err) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    int4 t = tet[e];
+    if (t.x < 0 || t.y < 0 || t.z < 0 || t.w < 0 || t.x >= nn || t.y >= nn || t.z >= nn || t.w >= nn)
+        atomicExch(err, 1);
+}
+
+__global__ void k_pack_tags_i32(const int32_t *__restrict__ src, int64_t ne, uint8_t *__restrict__ dst,
+                                int *__restrict__ maxtag, int *__restrict__ err) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    int32_t t = src[e];
+    if (t < 1 || t > kMaxMaterials) {
+        atomicExch(err, 1);
+        t = 1;
+    }
+    dst[e] = (uint8_t)t;
+    atomicMax(maxtag, t);
+}
+
+__global__ void k_pack_tags_f64(const double *__restrict__ src, int64_t ne, uint8_t *__restrict__ dst,
+                                int *__restrict__ maxtag, int *__restrict__ err) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    double v = src[e];
+    int t = (v >= 1.0 && v < 256.0) ? (int)v : 0;
+    if (t < 1 || t > kMaxMaterials) {
+        atomicExch(err, 1);
+        t = 1;
+    }
+    dst[e] = (uint8_t)t;
+    atomicMax(maxtag, t);
+}
+
+// Signs: bit k of signbits[e] set <=> sign -1. Counts disagreements with the
+// Mesh.m:134-135 rule so that matching signs need not be stored.
+__global__ void k_pack_signs_i8(const int8_t *__restrict__ s, const int4 *__restrict__ tet, int64_t ne,
+                                uint8_t *__restrict__ bits, int *__restrict__ mismatch,
+                                int *__restrict__ err) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    int4 t = tet[e];
+    int n[4] = {t.x, t.y, t.z, t.w};
+    unsigned b = 0, d = 0;
+    for (int k = 0; k < 6; k++) {
+        int8_t v = s[6 * e + k];
+        if (v != 1 && v != -1) atomicExch(err, 1);
+        b |= (v < 0 ? 1u : 0u) << k;
+        d |= (n[edge_a(k)] < n[edge_b(k)] ? 0u : 1u) << k;
+    }
+    bits[e] = (uint8_t)b;
+    if (b != d) atomicAdd(mismatch, 1);
+}
+
+__global__ void k_pack_signs_f64(const double *__restrict__ s, int64_t ne, uint8_t *__restrict__ bits,
+                                 int *__restrict__ err) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    unsigned b = 0;
+    for (int k = 0; k < 6; k++) {
+        double v = s[6 * e + k];
+        if (v != 1.0 && v != -1.0) atomicExch(err, 1);
+        b |= (v < 0 ? 1u : 0u) << k;
+    }
+    bits[e] = (uint8_t)b;
+}
+
+__global__ void k_check_geometry(const double4 *__restrict__ xyz, const int4 *__restrict__ tet,
+                                 int64_t ne, int *__restrict__ err) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    int4 t = tet[e];
+    double4 a = xyz[t.x], b = xyz[t.y], c = xyz[t.z], d = xyz[t.w];
+    double u0 = b.x - a.x, u1 = b.y - a.y, u2 = b.z - a.z;
+    double v0 = c.x - a.x, v1 = c.y - a.y, v2 = c.z - a.z;
+    double w0 = d.x - a.x, w1 = d.y - a.y, w2 = d.z - a.z;
+    double det = u0 * (v1 * w2 - w1 * v2) - v0 * (u1 * w2 - w1 * u2) + w0 * (u1 * v2 - v1 * u2);
+    if (!(det != 0.0) || !isfinite(det)) atomicExch(err, 1);
+}
+
+__global__ void k_i32_to_i64(const int32_t *__restrict__ a, int64_t n, int64_t *__restrict__ b) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+struct Dev {
+    void *p = nullptr;
+    cudaStream_t s = nullptr;
+    explicit Dev(cudaStream_t st) : s(st) {}
+    ~Dev() {
+        if (p) cudaFreeAsync(p, s);
+    }
+    cudaError_t alloc(size_t bytes) { return cudaMallocAsync(&p, bytes ? bytes : 16, s); }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+int sync_flag(const int *d, cudaStream_t s, int *h) {
+    MAG_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MAG_CUDA_TRY(cudaStreamSynchronize(s));
+    return MAG_OK;
+}
+
+// Order-2 Nedelec reference data of get_quadrature_data.m:18-28 and
+// nedelec_tet_p1.m:28-51, evaluated as those scripts do.
+void default_reference_data(double qw[4], double curl[72], double val[72]) {
+    const double a = 0.58541020, b = 0.13819660;
+    const double xi[4] = {a, b, b, b}, eta[4] = {b, a, b, b}, zeta[4] = {b, b, a, b};
+    const double G[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int q = 0; q < 4; q++) {
+        qw[q] = 1.0 / 24.0;
+        double L[4] = {((1.0 - xi[q]) - eta[q]) - zeta[q], xi[q], eta[q], zeta[q]};
+        for (int e = 0; e < 6; e++) {
+            int i = edge_a(e), j = edge_b(e);
+            double cr[3] = {G[i][1] * G[j][2] - G[i][2] * G[j][1], G[i][2] * G[j][0] - G[i][0] * G[j][2],
+                            G[i][0] * G[j][1] - G[i][1] * G[j][0]};
+            for (int c = 0; c < 3; c++) {
+                val[e + 6 * c + 18 * q] = G[j][c] * L[i] - G[i][c] * L[j];
+                curl[e + 6 * c + 18 * q] = 2.0 * cr[c];
+            }
+        }
+    }
+}
+
+bool is_standard_curl(const double *curl, int nq) {
+    static const double std_c[6][3] = {{0, -2, 2}, {2, 0, -2}, {-2, 2, 0}, {0, 0, 2}, {0, -2, 0}, {2, 0, 0}};
+    for (int q = 0; q < nq; q++)
+        for (int i = 0; i < 6; i++)
+            for (int c = 0; c < 3; c++)
+                if (curl[i + 6 * c + 18 * q] != std_c[i][c]) return false;
+    return true;
+}
+
+}  // namespace
+
+// Material tables on the device.
+struct MaterialStore {
+    void *mem = nullptr;
+    MaterialParams mp{};
+};
+
+int upload_materials(const double *lin, const double *isnon, const double *maxb, int nmat,
+                     const double *brk, int nbrk, const double *coe, int ncoe, const double *start,
+                     const double *cnt, const double *coestart, MaterialStore *out, cudaStream_t s) {
+    if (nmat <= 0 || !lin || !isnon || !maxb || !start || !cnt || !coestart || nbrk < 0 || ncoe < 0) {
+        set_error("materials: bad arguments");
+        return MAG_E_ARG;
+    }
+    // validate the spline windows on the host
+    for (int m = 0; m < nmat; m++) {
+        if (isnon[m] == 0.0) continue;
+        int st = (int)start[m], c = (int)cnt[m], cs = (int)coestart[m];
+        if (c < 1 || st < 0 || st + c > nbrk || cs < 0 || cs + 4 * c > ncoe) {
+            set_error("materials: spline table of tag %d out of range", m + 1);
+            return MAG_E_RANGE;
+        }
+    }
+    size_t nd = (size_t)3 * nmat + nbrk + ncoe, ni = (size_t)3 * nmat;
+    size_t bytes = nd * 8 + ni * 4 + 64;
+    char *host = new (std::nothrow) char[bytes];
+    if (!host) return MAG_E_NOMEM;
+    double *hd = reinterpret_cast<double *>(host);
+    std::memcpy(hd, lin, nmat * 8);
+    std::memcpy(hd + nmat, isnon, nmat * 8);
+    std::memcpy(hd + 2 * nmat, maxb, nmat * 8);
+    if (nbrk) std::memcpy(hd + 3 * nmat, brk, nbrk * 8);
+    if (ncoe) std::memcpy(hd + 3 * nmat + nbrk, coe, ncoe * 8);
+    int *hi = reinterpret_cast<int *>(hd + nd);
+    for (int m = 0; m < nmat; m++) {
+        hi[m] = (int)start[m];
+        hi[nmat + m] = (int)cnt[m];
+        hi[2 * nmat + m] = (int)coestart[m];
+    }
+    void *dmem = nullptr;
+    cudaError_t ce = cudaMalloc(&dmem, bytes);
+    if (ce != cudaSuccess) {
+        delete[] host;
+        set_error("materials: %s", cudaGetErrorString(ce));
+        return MAG_E_NOMEM;
+    }
+    ce = cudaMemcpyAsync(dmem, host, bytes, cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    delete[] host;
+    if (ce != cudaSuccess) {
+        cudaFree(dmem);
+        set_error("materials: %s", cudaGetErrorString(ce));
+        return MAG_E_CUDA;
+    }
+    if (out->mem) cudaFree(out->mem);
+    out->mem = dmem;
+    double *dd = static_cast<double *>(dmem);
+    int *di = reinterpret_cast<int *>(dd + nd);
+    out->mp = MaterialParams{nmat, nbrk, ncoe, dd, dd + nmat, dd + 2 * nmat, dd + 3 * nmat,
+                             dd + 3 * nmat + nbrk, di, di + nmat, di + 2 * nmat};
+    return MAG_OK;
+}
+
+int make_quad(const double *qw, int nq, const double *curl, const double *val, QuadParams *qp,
+              double **d_ref, cudaStream_t s) {
+    if (nq < 1 || nq > kMaxQuad || !qw || !curl || !val) {
+        set_error("quadrature: need 1..%d points and both basis tables", kMaxQuad);
+        return MAG_E_ARG;
+    }
+    QuadParams q{};
+    q.nq = nq;
+    q.uniform_w = 1;
+    for (int i = 0; i < nq; i++) {
+        q.qw[i] = qw[i];
+        if (qw[i] != qw[0]) q.uniform_w = 0;
+    }
+    q.standard_curl = is_standard_curl(curl, nq) ? 1 : 0;
+    double *d = nullptr;
+    MAG_CUDA_TRY(cudaMalloc(&d, 2 * 18 * nq * sizeof(double)));
+    cudaError_t ce = cudaMemcpyAsync(d, curl, 18 * nq * 8, cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(d + 18 * nq, val, 18 * nq * 8, cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) {
+        cudaFree(d);
+        set_error("quadrature: %s", cudaGetErrorString(ce));
+        return MAG_E_CUDA;
+    }
+    q.curl_ref = d;
+    q.val_ref = d + 18 * nq;
+    if (*d_ref) cudaFree(*d_ref);
+    *d_ref = d;
+    *qp = q;
+    return MAG_OK;
+}
+
+}  // namespace mag
+
+using namespace mag;
+
+struct mag_mesh {
+    int64_t nn = 0, ne = 0, ndof = 0;
+    double4 *xyz = nullptr;
+    int4 *tet = nullptr;
+    int32_t *dofs = nullptr;
+    uint8_t *tags = nullptr;
+    uint8_t *signbits = nullptr;
+    int max_tag = 0;
+    PatternBuffers pat;
+    double *scratch = nullptr;
+    QuadParams qp{};
+    double *d_ref = nullptr;
+    MaterialStore mat;
+    int has_mat = 0;
+    int64_t bytes = 0;
+
+    ElemData elems() const { return ElemData{xyz, tet, dofs, tags, signbits, ne}; }
+    RowPlan rows() const {
+        return RowPlan{pat.row_ptr, pat.inc_ptr, pat.inc_elem, pat.inc_pos, ndof, pat.wide};
+    }
+};
+
+namespace {
+
+void destroy_mesh(mag_mesh *m) {
+    if (!m) return;
+    void *ptrs[] = {m->xyz, m->tet, m->dofs, m->tags, m->signbits, m->scratch, m->d_ref, m->mat.mem};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    free_pattern(&m->pat, nullptr);
+    cudaDeviceSynchronize();
+    delete m;
+}
+
+int require_ready(const mag_mesh *m, bool need_mat) {
+    if (!m) {
+        set_error("null mesh handle");
+        return MAG_E_ARG;
+    }
+    if (need_mat && !m->has_mat) {
+        set_error("materials not set (mag_mesh_set_materials)");
+        return MAG_E_ARG;
+    }
+    if (need_mat && m->mat.mp.nmat < m->max_tag) {
+        set_error("material table has %d entries but the mesh uses tag %d", m->mat.mp.nmat, m->max_tag);
+        return MAG_E_RANGE;
+    }
+    return MAG_OK;
+}
+
+int finish(cudaStream_t s) {
+    (void)s;
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        set_error("kernel launch failed: %s", cudaGetErrorString(e));
+        return MAG_E_CUDA;
+    }
+    return MAG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mag_version(void) { return 1; }
+const char *mag_last_error(void) { return g_err; }
+
+int mag_generate_edges(const int32_t *d_T, int64_t Ne, int64_t Nn, int32_t *d_edges, int32_t *d_t2e,
+                       int8_t *d_sign, int64_t *E_out, void *stream) {
+    return generate_edges(d_T, Ne, Nn, d_edges, d_t2e, d_sign, E_out, (cudaStream_t)stream);
+}
+
+int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t Ne,
+                    const int32_t *d_dofs, const int8_t *d_signs, const int32_t *d_tags,
+                    int64_t num_dofs, mag_mesh **out, void *stream) {
+    if (!out || !d_P || !d_T || !d_dofs || !d_tags || Nn <= 0 || Ne <= 0 || num_dofs <= 0) {
+        set_error("mag_mesh_create: bad arguments");
+        return MAG_E_ARG;
+    }
+    *out = nullptr;
+    cudaStream_t s = (cudaStream_t)stream;
+    mag_mesh *m = new (std::nothrow) mag_mesh();
+    if (!m) return MAG_E_NOMEM;
+    m->nn = Nn;
+    m->ne = Ne;
+    m->ndof = num_dofs;
+    auto fail = [&](int code) {
+        destroy_mesh(m);
+        return code;
+    };
+    Dev err(s), mx(s), mism(s);
+    if (err.alloc(4) != cudaSuccess || mx.alloc(4) != cudaSuccess || mism.alloc(4) != cudaSuccess) {
+        set_error("mag_mesh_create: out of device memory");
+        return fail(MAG_E_NOMEM);
+    }
+    cudaMemsetAsync(err.p, 0, 4, s);
+    cudaMemsetAsync(mx.p, 0, 4, s);
+    cudaMemsetAsync(mism.p, 0, 4, s);
+    size_t b_xyz = Nn * sizeof(double4), b_tet = Ne * sizeof(int4), b_dofs = Ne * 6 * 4, b_tags = Ne;
+    if (cudaMalloc(&m->xyz, b_xyz) != cudaSuccess || cudaMalloc(&m->tet, b_tet) != cudaSuccess ||
+        cudaMalloc(&m->dofs, b_dofs) != cudaSuccess || cudaMalloc(&m->tags, b_tags) != cudaSuccess) {
+        set_error("mag_mesh_create: out of device memory");
+        return fail(MAG_E_NOMEM);
+    }
+    m->bytes = b_xyz + b_tet + b_dofs + b_tags;
+    k_pack_xyz<<<grid(Nn), kB, 0, s>>>(d_P, Nn, m->xyz, err.as<int>());
+    cudaMemcpyAsync(m->tet, d_T, b_tet, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(m->dofs, d_dofs, b_dofs, cudaMemcpyDeviceToDevice, s);
+    k_check_nodes<<<grid(Ne), kB, 0, s>>>(m->tet, Ne, Nn, err.as<int>());
+    int h = 0;
+    if (sync_flag(err.as<int>(), s, &h) != MAG_OK) return fail(MAG_E_CUDA);
+    if (h) {
+        set_error("mag_mesh_create: node id out of range or non-finite coordinate");
+        return fail(MAG_E_RANGE);
+    }
+    k_check_geometry<<<grid(Ne), kB, 0, s>>>(m->xyz, m->tet, Ne, err.as<int>());
+    if (sync_flag(err.as<int>(), s, &h) != MAG_OK) return fail(MAG_E_CUDA);
+    if (h) {
+        set_error("mag_mesh_create: degenerate element (zero or non-finite det J)");
+        return fail(MAG_E_GEOMETRY);
+    }
+    k_pack_tags_i32<<<grid(Ne), kB, 0, s>>>(d_tags, Ne, m->tags, mx.as<int>(), err.as<int>());
+    if (sync_flag(err.as<int>(), s, &h) != MAG_OK) return fail(MAG_E_CUDA);
+    if (h) {
+        set_error("mag_mesh_create: region tag outside 1..%d", kMaxMaterials);
+        return fail(MAG_E_RANGE);
+    }
+    if (sync_flag(mx.as<int>(), s, &m->max_tag) != MAG_OK) return fail(MAG_E_CUDA);
+    if (d_signs) {
+        if (cudaMalloc(&m->signbits, Ne) != cudaSuccess) return fail(MAG_E_NOMEM);
+        k_pack_signs_i8<<<grid(Ne), kB, 0, s>>>(d_signs, m->tet, Ne, m->signbits, mism.as<int>(),
+                                                err.as<int>());
+        int mm = 0;
+        if (sync_flag(err.as<int>(), s, &h) != MAG_OK || sync_flag(mism.as<int>(), s, &mm) != MAG_OK)
+            return fail(MAG_E_CUDA);
+        if (h) {
+            set_error("mag_mesh_create: signs must be +1 or -1");
+            return fail(MAG_E_ARG);
+        }
+        if (mm == 0) {  // identical to the derived rule: do not store them
+            cudaFree(m->signbits);
+            m->signbits = nullptr;
+        } else {
+            m->bytes += Ne;
+        }
+    }
+    int rc = build_pattern(m->dofs, Ne, num_dofs, &m->pat, s);
+    if (rc != MAG_OK) return fail(rc);
+    m->bytes += (int64_t)(num_dofs + 1) * 8 + m->pat.nnz * 4 + m->pat.ninc * 4 * (m->pat.wide ? 3 : 2);
+    if (cudaMalloc(&m->scratch, (size_t)Ne * kScratchPerElem * sizeof(double)) != cudaSuccess) {
+        set_error("mag_mesh_create: out of device memory for the element scratch");
+        return fail(MAG_E_NOMEM);
+    }
+    m->bytes += (int64_t)Ne * kScratchPerElem * 8;
+    double qw[4], curl[72], val[72];
+    default_reference_data(qw, curl, val);
+    rc = make_quad(qw, 4, curl, val, &m->qp, &m->d_ref, s);
+    if (rc != MAG_OK) return fail(rc);
+    *out = m;
+    return MAG_OK;
+}
+
+int mag_mesh_destroy(mag_mesh *mesh) {
+    destroy_mesh(mesh);
+    return MAG_OK;
+}
+
+int mag_mesh_get_info(const mag_mesh *m, mag_mesh_info *info) {
+    if (!m || !info) {
+        set_error("mag_mesh_get_info: bad arguments");
+        return MAG_E_ARG;
+    }
+    std::memset(info, 0, sizeof *info);
+    info->num_nodes = m->nn;
+    info->num_elements = m->ne;
+    info->num_dofs = m->ndof;
+    info->nnz = m->pat.nnz;
+    info->num_incidences = m->pat.ninc;
+    info->max_row_nnz = m->pat.max_row;
+    info->wide_positions = m->pat.wide;
+    info->signs_derived = m->signbits ? 0 : 1;
+    info->device_bytes = m->bytes;
+    return MAG_OK;
+}
+
+int mag_mesh_pattern(const mag_mesh *m, int64_t *d_row_ptr, int32_t *d_col_idx, void *stream) {
+    if (!m || !d_row_ptr || !d_col_idx) {
+        set_error("mag_mesh_pattern: bad arguments");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    k_i32_to_i64<<<grid(m->ndof + 1), kB, 0, s>>>(m->pat.row_ptr, m->ndof + 1, d_row_ptr);
+    MAG_CUDA_TRY(cudaMemcpyAsync(d_col_idx, m->pat.col_idx, m->pat.nnz * 4, cudaMemcpyDeviceToDevice, s));
+    return finish(s);
+}
+
+int mag_mesh_set_quadrature(mag_mesh *m, const double *qw, int nq, const double *curl_ref,
+                            const double *val_ref) {
+    if (!m) {
+        set_error("null mesh handle");
+        return MAG_E_ARG;
+    }
+    return make_quad(qw, nq, curl_ref, val_ref, &m->qp, &m->d_ref, nullptr);
+}
+
+int mag_mesh_set_materials(mag_mesh *m, const double *lin_nu, const double *is_nonlinear,
+                           const double *max_bsq, int nmat, const double *breaks, int nbreaks,
+                           const double *coefs, int ncoefs, const double *spline_start,
+                           const double *spline_count, const double *coef_start) {
+    if (!m) {
+        set_error("null mesh handle");
+        return MAG_E_ARG;
+    }
+    int rc = upload_materials(lin_nu, is_nonlinear, max_bsq, nmat, breaks, nbreaks, coefs, ncoefs,
+                              spline_start, spline_count, coef_start, &m->mat, nullptr);
+    if (rc == MAG_OK) m->has_mat = 1;
+    return rc;
+}
+
+int mag_assemble_jacobian(mag_mesh *m, const double *d_sol, double *d_vals, double *d_res, int calc_j,
+                          void *stream) {
+    MAG_TRY(require_ready(m, true));
+    if (!d_sol || !d_res || (calc_j && !d_vals)) {
+        set_error("mag_assemble_jacobian: bad arguments");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_TRY(launch_jacobian_elems(m->elems(), d_sol, m->qp, m->mat.mp, calc_j, m->scratch, s));
+    MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, calc_j ? d_vals : nullptr, d_res, s));
+    return finish(s);
+}
+
+int mag_assemble_stiffness(mag_mesh *m, const double *d_nu, double *d_vals, void *stream) {
+    MAG_TRY(require_ready(m, false));
+    if (!d_nu || !d_vals) {
+        set_error("mag_assemble_stiffness: bad arguments");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_TRY(launch_stiffness_elems(m->elems(), d_nu, m->qp, m->scratch, s));
+    MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, d_vals, nullptr, s));
+    return finish(s);
+}
+
+int mag_assemble_mass(mag_mesh *m, const double *d_sigma, double *d_vals, void *stream) {
+    MAG_TRY(require_ready(m, false));
+    if (!d_vals) {
+        set_error("mag_assemble_mass: bad arguments");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_TRY(launch_mass_elems(m->elems(), d_sigma, m->qp, m->scratch, s));
+    MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, d_vals, nullptr, s));
+    return finish(s);
+}
+
+int mag_assemble_source(mag_mesh *m, const double *d_js, double *d_out, void *stream) {
+    MAG_TRY(require_ready(m, false));
+    if (!d_js || !d_out) {
+        set_error("mag_assemble_source: bad arguments");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_TRY(launch_source_elems(m->elems(), d_js, m->qp, m->scratch, s));
+    MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, nullptr, d_out, s));
+    return finish(s);
+}
+
+int mag_element_b(mag_mesh *m, const double *d_sol, double *d_b, double *d_bsq, void *stream) {
+    MAG_TRY(require_ready(m, false));
+    if (!d_sol || (!d_b && !d_bsq)) {
+        set_error("mag_element_b: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (!m->qp.standard_curl) {
+        set_error("mag_element_b: needs the standard Nedelec curl table");
+        return MAG_E_UNSUPPORTED;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_TRY(launch_element_b(m->elems(), d_sol, d_b, d_bsq, s));
+    return finish(s);
+}
+
+int mag_csr_drop_zeros(const int64_t *d_row_ptr, const int32_t *d_col_idx, const double *d_vals,
+                       int64_t nrows, int64_t *d_row_ptr_out, int32_t *d_col_out, double *d_vals_out,
+                       int64_t *nnz_out, void *stream) {
+    return csr_drop_zeros(d_row_ptr, d_col_idx, d_vals, nrows, d_row_ptr_out, d_col_out, d_vals_out,
+                          nnz_out, (cudaStream_t)stream);
+}
+
+// ---- MEX-compatible entry points ------------------------------------------------
+
+namespace {
+
+struct MexMesh {
+    Dev xyz, tet, dofs, tags, signs, P, Td, Dd, Sd, Gd, scratch;
+    ElemData ed{};
+    explicit MexMesh(cudaStream_t s)
+        : xyz(s), tet(s), dofs(s), tags(s), signs(s), P(s), Td(s), Dd(s), Sd(s), Gd(s), scratch(s) {}
+};
+
+// Upload the reference's double arrays and convert them to the device layout.
+int mex_upload(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+               const double *Signs, const double *Tags, int64_t dof_limit, MexMesh &mm, int *max_tag,
+               cudaStream_t s) {
+    if (!P || !T || !Dofs || !Signs || Nn <= 0 || Ne <= 0) {
+        set_error("mex: bad arguments");
+        return MAG_E_ARG;
+    }
+    Dev err(s), mx(s);
+    MAG_CUDA_TRY(err.alloc(4));
+    MAG_CUDA_TRY(mx.alloc(4));
+    MAG_CUDA_TRY(cudaMemsetAsync(err.p, 0, 4, s));
+    MAG_CUDA_TRY(cudaMemsetAsync(mx.p, 0, 4, s));
+    MAG_CUDA_TRY(mm.P.alloc(Nn * 24));
+    MAG_CUDA_TRY(mm.Td.alloc(Ne * 32));
+    MAG_CUDA_TRY(mm.Dd.alloc(Ne * 48));
+    MAG_CUDA_TRY(mm.Sd.alloc(Ne * 48));
+    MAG_CUDA_TRY(mm.xyz.alloc(Nn * sizeof(double4)));
+    MAG_CUDA_TRY(mm.tet.alloc(Ne * 16));
+    MAG_CUDA_TRY(mm.dofs.alloc(Ne * 24));
+    MAG_CUDA_TRY(mm.tags.alloc(Ne));
+    MAG_CUDA_TRY(mm.signs.alloc(Ne));
+    MAG_CUDA_TRY(cudaMemcpyAsync(mm.P.p, P, Nn * 24, cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(mm.Td.p, T, Ne * 32, cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(mm.Dd.p, Dofs, Ne * 48, cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(mm.Sd.p, Signs, Ne * 48, cudaMemcpyHostToDevice, s));
+    k_pack_xyz<<<grid(Nn), kB, 0, s>>>(mm.P.as<double>(), Nn, mm.xyz.as<double4>(), err.as<int>());
+    k_index_from_double<<<grid(4 * Ne), kB, 0, s>>>(mm.Td.as<double>(), 4 * Ne, mm.tet.as<int32_t>(), Nn, 0,
+                                                    err.as<int>());
+    k_index_from_double<<<grid(6 * Ne), kB, 0, s>>>(mm.Dd.as<double>(), 6 * Ne, mm.dofs.as<int32_t>(),
+                                                    dof_limit, 1, err.as<int>());
+    k_pack_signs_f64<<<grid(Ne), kB, 0, s>>>(mm.Sd.as<double>(), Ne, mm.signs.as<uint8_t>(), err.as<int>());
+    if (Tags) {
+        MAG_CUDA_TRY(mm.Gd.alloc(Ne * 8));
+        MAG_CUDA_TRY(cudaMemcpyAsync(mm.Gd.p, Tags, Ne * 8, cudaMemcpyHostToDevice, s));
+        k_pack_tags_f64<<<grid(Ne), kB, 0, s>>>(mm.Gd.as<double>(), Ne, mm.tags.as<uint8_t>(), mx.as<int>(),
+                                                err.as<int>());
+    } else {
+        MAG_CUDA_TRY(cudaMemsetAsync(mm.tags.p, 1, Ne, s));
+    }
+    int h = 0;
+    MAG_TRY(sync_flag(err.as<int>(), s, &h));
+    if (h) {
+        set_error("mex: index, sign or tag out of range (nodes 1..Nn, dofs 0..numel(SolA), signs +-1, tags 1..255)");
+        return MAG_E_RANGE;
+    }
+    MAG_TRY(sync_flag(mx.as<int>(), s, max_tag));
+    mm.ed = ElemData{mm.xyz.as<double4>(), mm.tet.as<int4>(), mm.dofs.as<int32_t>(),
+                     mm.tags.as<uint8_t>(), mm.signs.as<uint8_t>(), Ne};
+    MAG_CUDA_TRY(mm.scratch.alloc((size_t)Ne * kScratchPerElem * 8));
+    return MAG_OK;
+}
+
+int mex_download(MexMesh &mm, int64_t Ne, int calcj, double *I, double *J, double *V, double *Ridx,
+                 double *Rval, cudaStream_t s) {
+    Dev out(s);
+    int64_t nk = calcj ? 36 * Ne : 0, nr = Ridx ? 6 * Ne : 0;
+    MAG_CUDA_TRY(out.alloc((3 * nk + 2 * nr) * 8));
+    double *dI = out.as<double>(), *dJ = dI + nk, *dV = dJ + nk, *dRi = dV + nk, *dRv = dRi + nr;
+    MAG_TRY(launch_to_triplets(mm.scratch.as<double>(), mm.dofs.as<int32_t>(), Ne, calcj, dI, dJ, dV,
+                               Ridx ? dRi : nullptr, Ridx ? dRv : nullptr, s));
+    if (nk) {
+        MAG_CUDA_TRY(cudaMemcpyAsync(I, dI, nk * 8, cudaMemcpyDeviceToHost, s));
+        MAG_CUDA_TRY(cudaMemcpyAsync(J, dJ, nk * 8, cudaMemcpyDeviceToHost, s));
+        MAG_CUDA_TRY(cudaMemcpyAsync(V, dV, nk * 8, cudaMemcpyDeviceToHost, s));
+    }
+    if (nr) {
+        MAG_CUDA_TRY(cudaMemcpyAsync(Ridx, dRi, nr * 8, cudaMemcpyDeviceToHost, s));
+        MAG_CUDA_TRY(cudaMemcpyAsync(Rval, dRv, nr * 8, cudaMemcpyDeviceToHost, s));
+    }
+    MAG_CUDA_TRY(cudaStreamSynchronize(s));
+    return MAG_OK;
+}
+
+}  // namespace
+
+int mag_mex_jacobian(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                     const double *Signs, const double *Tags, const double *SolA, int64_t Ndof,
+                     const double *Qw, int nq, const double *CurlRef, const double *lin,
+                     const double *isNon, const double *maxB, int nmat, const double *brk, int nbrk,
+                     const double *coe, int ncoe, const double *start, const double *cnt,
+                     const double *coeStart, int calc_j, double *I, double *J, double *V,
+                     double *R_idx, double *R_val) {
+    cudaStream_t s = nullptr;
+    if (!Tags || !SolA || Ndof <= 0 || !R_idx || !R_val || (calc_j && (!I || !J || !V))) {
+        set_error("mag_mex_jacobian: bad arguments");
+        return MAG_E_ARG;
+    }
+    MexMesh mm(s);
+    int max_tag = 0;
+    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, Tags, Ndof, mm, &max_tag, s));
+    MaterialStore ms;
+    MAG_TRY(upload_materials(lin, isNon, maxB, nmat, brk, nbrk, coe, ncoe, start, cnt, coeStart, &ms, s));
+    struct Guard {
+        MaterialStore &m;
+        double *q = nullptr;
+        ~Guard() {
+            if (m.mem) cudaFree(m.mem);
+            if (q) cudaFree(q);
+        }
+    } guard{ms};
+    if (nmat < max_tag) {
+        set_error("mag_mex_jacobian: tag %d has no material entry", max_tag);
+        return MAG_E_RANGE;
+    }
+    QuadParams qp{};
+    // the Jacobian kernel takes no basis values; reuse the curl table for the slot
+    MAG_TRY(make_quad(Qw, nq, CurlRef, CurlRef, &qp, &guard.q, s));
+    // dofs must index SolA
+    Dev sol(s);
+    MAG_CUDA_TRY(sol.alloc(Ndof * 8));
+    MAG_CUDA_TRY(cudaMemcpyAsync(sol.p, SolA, Ndof * 8, cudaMemcpyHostToDevice, s));
+    MAG_TRY(launch_jacobian_elems(mm.ed, sol.as<double>(), qp, ms.mp, calc_j, mm.scratch.as<double>(), s));
+    return mex_download(mm, Ne, calc_j, I, J, V, R_idx, R_val, s);
+}
+
+int mag_mex_curl_curl(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                      const double *Signs, const double *Nu, const double *Qw, int nq,
+                      const double *CurlRef, double *I, double *J, double *V) {
+    cudaStream_t s = nullptr;
+    if (!Nu || !I || !J || !V) {
+        set_error("mag_mex_curl_curl: bad arguments");
+        return MAG_E_ARG;
+    }
+    MexMesh mm(s);
+    int max_tag = 0;
+    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, (int64_t)1 << 31, mm, &max_tag, s));
+    QuadParams qp{};
+    double *dq = nullptr;
+    MAG_TRY(make_quad(Qw, nq, CurlRef, CurlRef, &qp, &dq, s));
+    Dev nu(s);
+    MAG_CUDA_TRY(nu.alloc(Ne * 8));
+    MAG_CUDA_TRY(cudaMemcpyAsync(nu.p, Nu, Ne * 8, cudaMemcpyHostToDevice, s));
+    int rc = launch_stiffness_elems(mm.ed, nu.as<double>(), qp, mm.scratch.as<double>(), s);
+    if (rc == MAG_OK) rc = mex_download(mm, Ne, 1, I, J, V, nullptr, nullptr, s);
+    cudaFree(dq);
+    return rc;
+}
+
+int mag_mex_mass(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                 const double *Signs, const double *Coeffs, int64_t ncoeffs, const double *Qw, int nq,
+                 const double *ValRef, double *I, double *J, double *V) {
+    cudaStream_t s = nullptr;
+    if (!I || !J || !V) {
+        set_error("mag_mex_mass: bad arguments");
+        return MAG_E_ARG;
+    }
+    MexMesh mm(s);
+    int max_tag = 0;
+    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, (int64_t)1 << 31, mm, &max_tag, s));
+    QuadParams qp{};
+    double *dq = nullptr;
+    MAG_TRY(make_quad(Qw, nq, ValRef, ValRef, &qp, &dq, s));
+    Dev sg(s);
+    const double *dsig = nullptr;
+    if (Coeffs && ncoeffs == Ne) {  // otherwise sigma = 1 (assemble_mass_kernel_mex.cpp:155)
+        MAG_CUDA_TRY(sg.alloc(Ne * 8));
+        MAG_CUDA_TRY(cudaMemcpyAsync(sg.p, Coeffs, Ne * 8, cudaMemcpyHostToDevice, s));
+        dsig = sg.as<double>();
+    }
+    int rc = launch_mass_elems(mm.ed, dsig, qp, mm.scratch.as<double>(), s);
+    if (rc == MAG_OK) rc = mex_download(mm, Ne, 1, I, J, V, nullptr, nullptr, s);
+    cudaFree(dq);
+    return rc;
+}
+
+}  // extern "C"

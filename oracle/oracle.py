@@ -1,0 +1,250 @@
+"""Python access to the oracle (TEST INFRASTRUCTURE ONLY).
+
+Two CPU implementations of the reference's element-assembly path:
+
+* ``RefMex`` -- the reference's own MEX kernels (src/mex/assemble_*_kernel_mex.cpp)
+  compiled unchanged into oracle/_ref/libref_mex.so by oracle/Makefile.
+* ``Port``   -- the C restatement in oracle/port (libmagoracle.so), which also
+  restates Mesh.generateEdges, MATLAB sparse() and pchip.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker or the timed CPU baseline; the product path
+never imports it. Inputs follow the reference's MEX boundary (Assembler.m):
+column-major doubles with 1-based indices.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libref_mex.so")
+PORT_SO = os.path.join(HERE, "libmagoracle.so")
+
+_dp = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_i8p = C.POINTER(C.c_int8)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def build(quiet: bool = True) -> None:
+    """Build the oracle libraries (make -C oracle)."""
+    import subprocess
+
+    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+
+
+@dataclass
+class MexInputs:
+    """Arguments exactly as Assembler.m passes them to the MEX gateways."""
+
+    P: np.ndarray      # [3 x Nn] doubles (stored (Nn,3) C-order)
+    T: np.ndarray      # [4 x Ne] 1-based doubles
+    Dofs: np.ndarray   # [6 x Ne] 1-based doubles
+    Signs: np.ndarray  # [6 x Ne] +-1 doubles
+    Tags: np.ndarray   # [Ne] doubles
+
+    @property
+    def ne(self):
+        return self.T.shape[0]
+
+    @property
+    def nn(self):
+        return self.P.shape[0]
+
+
+def mex_inputs(P, T0, t2e0, sign, tags) -> MexInputs:
+    """Convert 0-based int mesh arrays to the reference's double/1-based layout."""
+    return MexInputs(P=_f64(P), T=_f64(np.asarray(T0) + 1), Dofs=_f64(np.asarray(t2e0) + 1),
+                     Signs=_f64(sign), Tags=_f64(tags))
+
+
+class _Lib:
+    def __init__(self, path):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(path)
+
+
+class Port(_Lib):
+    """The C restatement (oracle/port)."""
+
+    def __init__(self, path: str = PORT_SO):
+        super().__init__(path)
+        L = self.lib
+        L.oracle_generate_edges.restype = C.c_int64
+        L.oracle_sparse_csr.restype = C.c_int64
+        L.oracle_sparse_vec.restype = C.c_int
+        L.oracle_pchip.restype = C.c_int
+
+    def generate_edges(self, T0: np.ndarray):
+        """Mesh.generateEdges on a 0-based (Ne,4) int array -> 0-based edges, t2e, sign."""
+        T1 = np.ascontiguousarray(T0, dtype=np.int32) + 1
+        ne = T1.shape[0]
+        cap = 6 * ne
+        edges = np.zeros((cap, 2), dtype=np.int32)
+        t2e = np.zeros((ne, 6), dtype=np.int32)
+        sign = np.zeros((ne, 6), dtype=np.int8)
+        E = self.lib.oracle_generate_edges(T1.ctypes.data_as(_i32p), C.c_int64(ne),
+                                           edges.ctypes.data_as(_i32p), C.c_int64(cap),
+                                           t2e.ctypes.data_as(_i32p), sign.ctypes.data_as(_i8p))
+        return edges[:E] - 1, t2e - 1, sign
+
+    def jacobian(self, m: MexInputs, sol, qw, curl, packed, calc_j=True):
+        ne = m.ne
+        nK = 36 * ne if calc_j else 0
+        I, J, V = (np.zeros(max(nK, 1)) for _ in range(3))
+        Ri, Rv = np.zeros(6 * ne), np.zeros(6 * ne)
+        pk = [_f64(a) for a in packed.as_tuple()]
+        sol, qw, curl = _f64(sol), _f64(qw), _f64(curl)
+        self.lib.oracle_jacobian(_d(m.P), _d(m.T), C.c_int64(ne), _d(m.Dofs), _d(m.Signs),
+                                 _d(m.Tags), _d(sol), _d(qw), C.c_int(qw.size), _d(curl),
+                                 *[_d(a) for a in pk], C.c_int(int(calc_j)), _d(I), _d(J), _d(V),
+                                 _d(Ri), _d(Rv))
+        return I[:nK], J[:nK], V[:nK], Ri, Rv
+
+    def curl_curl(self, m: MexInputs, nu, qw, curl):
+        ne = m.ne
+        I, J, V = (np.zeros(36 * ne) for _ in range(3))
+        nu, qw, curl = _f64(nu), _f64(qw), _f64(curl)
+        self.lib.oracle_curl_curl(_d(m.P), _d(m.T), C.c_int64(ne), _d(m.Dofs), _d(m.Signs),
+                                  _d(nu), _d(qw), C.c_int(qw.size), _d(curl), _d(I), _d(J), _d(V))
+        return I, J, V
+
+    def mass(self, m: MexInputs, coeffs, qw, val):
+        ne = m.ne
+        I, J, V = (np.zeros(36 * ne) for _ in range(3))
+        qw, val = _f64(qw), _f64(val)
+        cf = None if coeffs is None else _f64(coeffs)
+        ncf = 0 if cf is None else cf.size
+        self.lib.oracle_mass(_d(m.P), _d(m.T), C.c_int64(ne), _d(m.Dofs), _d(m.Signs), _d(cf),
+                             C.c_int64(ncf), _d(qw), C.c_int(qw.size), _d(val), _d(I), _d(J), _d(V))
+        return I, J, V
+
+    def source(self, m: MexInputs, js, qw, val):
+        ne = m.ne
+        I, V = np.zeros(6 * ne), np.zeros(6 * ne)
+        js, qw, val = _f64(js), _f64(qw), _f64(val)
+        self.lib.oracle_source(_d(m.P), _d(m.T), C.c_int64(ne), _d(m.Dofs), _d(m.Signs), _d(js),
+                               _d(qw), C.c_int(qw.size), _d(val), _d(I), _d(V))
+        return I, V
+
+    def sparse_csr(self, I, J, V, N, drop_zeros=True):
+        I, J, V = _f64(I), _f64(J), _f64(V)
+        n = I.size
+        nnz = self.lib.oracle_sparse_csr(_d(I), _d(J), _d(V), C.c_int64(n), C.c_int64(N),
+                                         C.c_int(int(drop_zeros)), None, None, None)
+        if nnz < 0:
+            raise ValueError("sparse: index out of range")
+        rp = np.zeros(N + 1, dtype=np.int64)
+        ci = np.zeros(max(nnz, 1), dtype=np.int32)
+        vv = np.zeros(max(nnz, 1))
+        self.lib.oracle_sparse_csr(_d(I), _d(J), _d(V), C.c_int64(n), C.c_int64(N),
+                                   C.c_int(int(drop_zeros)), rp.ctypes.data_as(_i64p),
+                                   ci.ctypes.data_as(_i32p), _d(vv))
+        return rp, ci[:nnz], vv[:nnz]
+
+    def sparse_vec(self, Ridx, Rval, N):
+        Ridx, Rval = _f64(Ridx), _f64(Rval)
+        out = np.zeros(N)
+        if self.lib.oracle_sparse_vec(_d(Ridx), _d(Rval), C.c_int64(Ridx.size), C.c_int64(N),
+                                      _d(out)) != 0:
+            raise ValueError("sparse vector: index out of range")
+        return out
+
+    def pchip(self, x, y):
+        x, y = _f64(x), _f64(y)
+        coefs = np.zeros((x.size - 1, 4))
+        if self.lib.oracle_pchip(_d(x), _d(y), C.c_int64(x.size), _d(coefs)) != 0:
+            raise ValueError("pchip failed")
+        return coefs
+
+
+class RefMex(_Lib):
+    """The reference's own MEX kernels, compiled unchanged (oracle/_ref)."""
+
+    def __init__(self, path: str = REF_SO):
+        super().__init__(path)
+        L = self.lib
+        for f in ("ref_jacobian", "ref_curl_curl", "ref_mass", "ref_source"):
+            getattr(L, f).restype = C.c_int
+        L.ref_last_error.restype = C.c_char_p
+        self.last_seconds = 0.0
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def jacobian(self, m: MexInputs, sol, qw, curl, packed, calc_j=True):
+        ne = m.ne
+        nK = 36 * ne if calc_j else 0
+        I, J, V = (np.empty(max(nK, 1)) for _ in range(3))
+        Ri, Rv = np.empty(6 * ne), np.empty(6 * ne)
+        pk = [_f64(a) for a in packed.as_tuple()]
+        sol, qw, curl = _f64(sol), _f64(qw), _f64(curl)
+        secs = C.c_double(0)
+        nmat = pk[0].size
+        rc = self.lib.ref_jacobian(
+            _d(m.P), C.c_size_t(m.nn), _d(m.T), C.c_size_t(ne), _d(m.Dofs), _d(m.Signs),
+            _d(m.Tags), _d(sol), C.c_size_t(sol.size), _d(qw), C.c_size_t(qw.size), _d(curl),
+            _d(pk[0]), _d(pk[1]), _d(pk[2]), C.c_size_t(nmat), _d(pk[3]), C.c_size_t(pk[3].size),
+            _d(pk[4]), C.c_size_t(pk[4].size), _d(pk[5]), _d(pk[6]), _d(pk[7]),
+            C.c_int(int(calc_j)), _d(I), _d(J), _d(V), _d(Ri), _d(Rv), C.byref(secs))
+        self._check(rc)
+        self.last_seconds = secs.value
+        return I[:nK], J[:nK], V[:nK], Ri, Rv
+
+    def curl_curl(self, m: MexInputs, nu, qw, curl):
+        ne = m.ne
+        I, J, V = (np.empty(36 * ne) for _ in range(3))
+        nu, qw, curl = _f64(nu), _f64(qw), _f64(curl)
+        secs = C.c_double(0)
+        rc = self.lib.ref_curl_curl(_d(m.P), C.c_size_t(m.nn), _d(m.T), C.c_size_t(ne), _d(m.Dofs),
+                                    _d(m.Signs), _d(nu), _d(qw), C.c_size_t(qw.size), _d(curl),
+                                    _d(I), _d(J), _d(V), C.byref(secs))
+        self._check(rc)
+        self.last_seconds = secs.value
+        return I, J, V
+
+    def mass(self, m: MexInputs, coeffs, qw, val):
+        ne = m.ne
+        I, J, V = (np.empty(36 * ne) for _ in range(3))
+        qw, val = _f64(qw), _f64(val)
+        cf = None if coeffs is None else _f64(coeffs)
+        secs = C.c_double(0)
+        rc = self.lib.ref_mass(_d(m.P), C.c_size_t(m.nn), _d(m.T), C.c_size_t(ne), _d(m.Dofs),
+                               _d(m.Signs), _d(cf), C.c_size_t(0 if cf is None else cf.size),
+                               _d(qw), C.c_size_t(qw.size), _d(val), _d(I), _d(J), _d(V),
+                               C.byref(secs))
+        self._check(rc)
+        self.last_seconds = secs.value
+        return I, J, V
+
+    def source(self, m: MexInputs, js, qw, val):
+        ne = m.ne
+        I, V = np.empty(6 * ne), np.empty(6 * ne)
+        js, qw, val = _f64(js), _f64(qw), _f64(val)
+        secs = C.c_double(0)
+        rc = self.lib.ref_source(_d(m.P), C.c_size_t(m.nn), _d(m.T), C.c_size_t(ne), _d(m.Dofs),
+                                 _d(m.Signs), _d(js), _d(qw), C.c_size_t(qw.size), _d(val),
+                                 _d(I), _d(V), C.byref(secs))
+        self._check(rc)
+        self.last_seconds = secs.value
+        return I, V
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)

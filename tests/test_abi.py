@@ -1,0 +1,50 @@
+"""The C-ABI library loads and exports every entry point include/magasm.h declares.
+
+CPU only: loading libmagasm.so makes no CUDA call, so this runs without a GPU.
+"""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+from magpackage_b200 import _lib
+
+HEADER_DIR = os.path.join(ROOT, "include")
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(HEADER_DIR):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(HEADER_DIR, fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(mag_\w+)\s*\(", text, re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_built_for_sm100a():
+    assert os.path.exists(_lib.LIB_PATH), "build libmagasm.so first (magpackage_b200/build.py)"
+
+
+def test_every_declared_symbol_is_exported():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    names = declared_symbols()
+    assert len(names) >= 15
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_header():
+    assert set(_lib.exported_symbols()) == declared_symbols()
+
+
+def test_version_and_error_text_without_gpu():
+    lib = _lib.load()
+    assert lib.mag_version() >= 1
+    assert isinstance(lib.mag_last_error(), bytes)
+    # argument validation happens before any CUDA call
+    rc = lib.mag_mesh_get_info(None, None)
+    assert rc == -1 and b"bad arguments" in lib.mag_last_error()

@@ -1,0 +1,349 @@
+"""GPU parity: the sm_100a path against the oracle, bit for bit.
+
+Every CSR produced on the GPU is compared with the oracle's restatement of
+MATLAB's sparse() applied to the reference MEX triplets (the compiled
+reference when oracle/_ref is present, its pinned C restatement otherwise):
+row_ptr/col_idx must be identical and every value identical bit for bit
+(tolerance 0; the north-star bound is 1e-12 relative per nonzero).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+from conftest import bits_equal, load_golden, packed_from_golden
+
+from magpackage_b200 import _lib, material, quadrature, synth
+from magpackage_b200.assembler import Assembler, DofHandler, Mesh
+from magpackage_b200.plan import AssemblyPlan, generate_edges
+from oracle.oracle import mex_inputs
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-12  # north-star bound per nonzero; the tests below demand exact equality
+
+
+def dev(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+def make_case(port, P, T, tags):
+    edges, t2e, sign = port.generate_edges(T)
+    return edges, t2e, sign, mex_inputs(P, T, t2e, sign, tags)
+
+
+def oracle_matrix(port, I, J, V, n, drop):
+    return port.sparse_csr(I, J, V, n, drop_zeros=drop)
+
+
+def assert_csr_equal(rp, ci, vals, ref):
+    rrp, rci, rv = ref
+    assert np.array_equal(host(rp), rrp), "row_ptr differs"
+    assert np.array_equal(host(ci), rci), "col_idx differs"
+    v = host(vals)
+    assert bits_equal(v, rv), f"values differ: max rel {np.max(np.abs(v - rv) / np.maximum(np.abs(rv), 1e-300))}"
+
+
+# ---- topology ----------------------------------------------------------------------
+
+@pytest.mark.parametrize("n", [1, 3, 8])
+def test_generate_edges_matches_oracle(oracle_port, n):
+    mesh = synth.kuhn_box(n, n + 1, max(n - 1, 1), seed=n)
+    edges, t2e, sign = generate_edges(mesh.T)
+    e0, t0, s0 = oracle_port.generate_edges(mesh.T)
+    assert np.array_equal(host(edges), e0) and np.array_equal(host(t2e), t0) and np.array_equal(host(sign), s0)
+
+
+def test_generate_edges_rejects_bad_nodes():
+    T = np.array([[0, 1, 2, 2]], dtype=np.int32)  # repeated node
+    with pytest.raises(_lib.MagError):
+        generate_edges(T)
+
+
+# ---- golden fixtures through the handle path ------------------------------------------
+
+@pytest.mark.parametrize("name", ["one_hex", "cube3"])
+def test_jacobian_matches_golden(oracle_port, name):
+    d = load_golden(name)
+    E = d["edges"].shape[0]
+    plan = AssemblyPlan(d["P"], d["T0"], d["t2e"], E, d["tags"], d["sign"])
+    assert plan.info.signs_derived == 1
+    plan.set_materials(packed_from_golden(d))
+    vals, res = plan.jacobian(dev(d["sol"]))
+    ref = oracle_matrix(oracle_port, d["jac_I"], d["jac_J"], d["jac_V"], E, drop=False)
+    assert_csr_equal(plan.row_ptr, plan.col_idx, vals, ref)
+    assert bits_equal(host(res), oracle_port.sparse_vec(d["jac_Ridx"], d["jac_Rval"], E))
+    # residual-only pass (CalcJ = false)
+    _, res0 = plan.jacobian(dev(d["sol"]), calc_j=False)
+    assert bits_equal(host(res0), oracle_port.sparse_vec(d["res_only_Ridx"], d["res_only_Rval"], E))
+    # MATLAB storage: exact zeros dropped
+    rp2, ci2, v2 = plan.drop_zeros(vals)
+    assert_csr_equal(rp2, ci2, v2, oracle_matrix(oracle_port, d["jac_I"], d["jac_J"], d["jac_V"], E, True))
+
+
+@pytest.mark.parametrize("name", ["one_hex", "cube3"])
+def test_stiffness_mass_source_match_golden(oracle_port, name):
+    d = load_golden(name)
+    E = d["edges"].shape[0]
+    plan = AssemblyPlan(d["P"], d["T0"], d["t2e"], E, d["tags"], d["sign"])
+    I, J = d["jac_I"], d["jac_J"]
+    k = plan.stiffness(dev(d["cc_nu"]))
+    assert_csr_equal(plan.row_ptr, plan.col_idx, k, oracle_matrix(oracle_port, I, J, d["cc_V"], E, False))
+    m = plan.mass(dev(d["mass_sigma"]))
+    assert_csr_equal(plan.row_ptr, plan.col_idx, m, oracle_matrix(oracle_port, I, J, d["mass_V"], E, False))
+    rp2, ci2, v2 = plan.drop_zeros(m)
+    assert_csr_equal(rp2, ci2, v2, oracle_matrix(oracle_port, I, J, d["mass_V"], E, True))
+    m1 = plan.mass(None)
+    assert_csr_equal(plan.row_ptr, plan.col_idx, m1, oracle_matrix(oracle_port, I, J, d["mass1_V"], E, False))
+    f = plan.source(dev(d["src_js"]))
+    assert bits_equal(host(f), oracle_port.sparse_vec(d["src_I"], d["src_V"], E))
+
+
+def test_unit_tet_known_answer_on_gpu():
+    """tests/test_mex_assembly.m:32-73 through the MEX-compatible entry point."""
+    d = load_golden("unit_tet")
+    L = _lib.lib()
+    P = np.ascontiguousarray(d["P"])
+    T = np.array([1.0, 2, 3, 4])
+    dofs = np.arange(1.0, 7.0)
+    signs = np.array([1.0, -1, 1, -1, 1, -1])
+    nu = np.array([500.0])
+    I, J, V = np.zeros(36), np.zeros(36), np.zeros(36)
+    qw, curl = np.ascontiguousarray(d["qw"]), np.ascontiguousarray(d["curl"])
+    _lib.check(L.mag_mex_curl_curl(_lib.dptr(P), 4, _lib.dptr(T), 1, _lib.dptr(dofs), _lib.dptr(signs),
+                                   _lib.dptr(nu), _lib.dptr(qw), qw.size, _lib.dptr(curl), _lib.dptr(I),
+                                   _lib.dptr(J), _lib.dptr(V)))
+    assert bits_equal(V, d["V"]) and bits_equal(I, d["I"]) and bits_equal(J, d["J"])
+
+
+@pytest.mark.parametrize("name", ["one_hex", "cube3"])
+def test_mex_entry_points_match_golden(name):
+    d = load_golden(name)
+    L = _lib.lib()
+    m = mex_inputs(d["P"], d["T0"], d["t2e"], d["sign"], d["tags"])
+    ne, nn, E = m.ne, m.nn, d["edges"].shape[0]
+    pk = [np.ascontiguousarray(a, dtype=np.float64) for a in packed_from_golden(d).as_tuple()]
+    qw, curl, val = (np.ascontiguousarray(d[k]) for k in ("qw", "curl", "val"))
+    sol = np.ascontiguousarray(d["sol"])
+    for cj in (1, 0):
+        I, J, V = (np.zeros(36 * ne) for _ in range(3))
+        Ri, Rv = np.zeros(6 * ne), np.zeros(6 * ne)
+        p = _lib.dptr
+        _lib.check(L.mag_mex_jacobian(p(m.P), nn, p(m.T), ne, p(m.Dofs), p(m.Signs), p(m.Tags), p(sol), E,
+                                      p(qw), qw.size, p(curl), p(pk[0]), p(pk[1]), p(pk[2]), pk[0].size,
+                                      p(pk[3]), pk[3].size, p(pk[4]), pk[4].size, p(pk[5]), p(pk[6]),
+                                      p(pk[7]), cj, p(I), p(J), p(V), p(Ri), p(Rv)))
+        if cj:
+            assert bits_equal(I, d["jac_I"]) and bits_equal(J, d["jac_J"]) and bits_equal(V, d["jac_V"])
+            assert bits_equal(Ri, d["jac_Ridx"]) and bits_equal(Rv, d["jac_Rval"])
+        else:
+            assert bits_equal(Rv, d["res_only_Rval"])
+    I, J, V = (np.zeros(36 * ne) for _ in range(3))
+    nu = np.ascontiguousarray(d["cc_nu"])
+    _lib.check(L.mag_mex_curl_curl(p(m.P), nn, p(m.T), ne, p(m.Dofs), p(m.Signs), p(nu), p(qw), qw.size,
+                                   p(curl), p(I), p(J), p(V)))
+    assert bits_equal(V, d["cc_V"])
+    sig = np.ascontiguousarray(d["mass_sigma"])
+    _lib.check(L.mag_mex_mass(p(m.P), nn, p(m.T), ne, p(m.Dofs), p(m.Signs), p(sig), ne, p(qw), qw.size,
+                              p(val), p(I), p(J), p(V)))
+    assert bits_equal(V, d["mass_V"])
+    _lib.check(L.mag_mex_mass(p(m.P), nn, p(m.T), ne, p(m.Dofs), p(m.Signs), None, 0, p(qw), qw.size,
+                              p(val), p(I), p(J), p(V)))
+    assert bits_equal(V, d["mass1_V"])
+
+
+# ---- fresh seeded meshes against the live oracle ------------------------------------------
+
+def _nonlinear_case(oracle_port, n, seed, scale=0.02):
+    mesh = synth.kuhn_box(n, seed=seed)
+    tags = synth.cube_layout(mesh)
+    edges, t2e, sign, m = make_case(oracle_port, mesh.P, mesh.T, tags)
+    E = edges.shape[0]
+    rng = np.random.default_rng(seed)
+    sol = rng.normal(0, scale, E) * 10.0 ** rng.uniform(-1.5, 0.5, E)
+    return mesh, tags, edges, t2e, sign, m, E, sol
+
+
+@pytest.mark.parametrize("n,seed", [(6, 1), (13, 2)])
+def test_jacobian_random_meshes(oracle_port, n, seed):
+    mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, n, seed)
+    qw, val, curl = quadrature.reference_data(2)
+    pk = material.pack_material_data(synth.standard_materials())
+    I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, qw, curl, pk, True)
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
+    plan.set_materials(pk)
+    vals, res = plan.jacobian(dev(sol))
+    assert_csr_equal(plan.row_ptr, plan.col_idx, vals, oracle_matrix(oracle_port, I, J, V, E, False))
+    assert bits_equal(host(res), oracle_port.sparse_vec(Ri, Rv, E))
+    assert plan.nnz == 115 * n ** 3 + 45 * n ** 2 + 3 * n
+
+
+def test_config1_assembler_surface(oracle_port):
+    """Config 1 (20^3 cube): K(nu) and M(sigma) through the Assembler mirror, MATLAB storage."""
+    mesh_s = synth.kuhn_box(20, seed=0)
+    tags = synth.cube_layout(mesh_s)
+    mesh = Mesh(mesh_s.P, mesh_s.T, tags)
+    dh = DofHandler(mesh)
+    dh.distribute_dofs()
+    asm = Assembler(mesh, dh)
+    nu_map = {synth.AIR: material.NU0, synth.IRON: material.NU0 / 1000.0, synth.ALUMINIUM: material.NU0}
+    sig_map = {synth.ALUMINIUM: synth.SIGMA_AL}
+    K = asm.assemble_stiffness(nu_map)
+    M = asm.assemble_mass_weighted(sig_map)
+    e0, t0, s0 = oracle_port.generate_edges(mesh_s.T)
+    m = mex_inputs(mesh_s.P, mesh_s.T, t0, s0, tags)
+    qw, val, curl = quadrature.reference_data(2)
+    E = e0.shape[0]
+    assert E == 59660 and dh.NumGlobalDofs == E
+    Ik, Jk, Vk = oracle_port.curl_curl(m, asm.expand_material_map(nu_map), qw, curl)
+    assert_csr_equal(K.row_ptr, K.col_idx, K.values, oracle_matrix(oracle_port, Ik, Jk, Vk, E, True))
+    Im, Jm, Vm = oracle_port.mass(m, asm.expand_material_map(sig_map), qw, val)
+    assert_csr_equal(M.row_ptr, M.col_idx, M.values, oracle_matrix(oracle_port, Im, Jm, Vm, E, True))
+    assert M.nnz < K.nnz  # only rows touching aluminium survive zero dropping
+
+
+def test_reduced_domain_dofs(oracle_port):
+    """DofHandler.distributeDofs with target regions: dofs only on active edges (DofHandler.m:72-105)."""
+    mesh_s = synth.kuhn_box(7, seed=3)
+    tags = synth.cube_layout(mesh_s)
+    mesh = Mesh(mesh_s.P, mesh_s.T, tags)
+    dh = DofHandler(mesh)
+    dofs = host(dh.distribute_dofs(target_region_tags=[synth.IRON, synth.ALUMINIUM]))
+    assert (dofs < 0).any() and dh.NumGlobalDofs < mesh.Edges.shape[0]
+    sign = host(mesh.T2E_Sign)
+    m = mex_inputs(mesh_s.P, mesh_s.T, dofs, sign, tags)
+    sol = np.random.default_rng(0).normal(0, 0.02, dh.NumGlobalDofs)
+    qw, val, curl = quadrature.reference_data(2)
+    pk = material.pack_material_data(synth.standard_materials())
+    I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, qw, curl, pk, True)
+    asm = Assembler(mesh, dh, matlab_storage=True)
+    Jm, R = asm.assemble_jacobian(sol, synth.standard_materials())
+    assert_csr_equal(Jm.row_ptr, Jm.col_idx, Jm.values, oracle_matrix(oracle_port, I, J, V, dh.NumGlobalDofs, True))
+    assert bits_equal(host(R), oracle_port.sparse_vec(Ri, Rv, dh.NumGlobalDofs))
+
+
+def test_generic_quadrature_path(oracle_port):
+    """Non-standard curl table and non-uniform weights take the general per-point loop."""
+    mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, 4, 5)
+    qw = np.array([0.05, 0.04, 0.045, 0.0316666])
+    _, val, curl = quadrature.reference_data(2)
+    curl = curl.copy()
+    curl[18 * 2: 18 * 3] *= 0.5  # one point with a scaled curl
+    pk = material.pack_material_data(synth.standard_materials())
+    I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, qw, curl, pk, True)
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
+    plan.set_quadrature(qw, curl, val)
+    plan.set_materials(pk)
+    vals, res = plan.jacobian(dev(sol))
+    assert_csr_equal(plan.row_ptr, plan.col_idx, vals, oracle_matrix(oracle_port, I, J, V, E, False))
+    assert bits_equal(host(res), oracle_port.sparse_vec(Ri, Rv, E))
+    nu = np.random.default_rng(1).uniform(1e2, 1e6, mesh.num_elements)
+    _, _, Vk = oracle_port.curl_curl(m, nu, qw, curl)
+    k = plan.stiffness(dev(nu))
+    assert_csr_equal(plan.row_ptr, plan.col_idx, k, oracle_matrix(oracle_port, I, J, Vk, E, False))
+    # uniform weights with the standard table take the fast path; same bits as the oracle
+    qw2, val2, curl2 = quadrature.reference_data(2)
+    plan.set_quadrature(qw2, curl2, val2)
+    vals2, _ = plan.jacobian(dev(sol))
+    I2, J2, V2, _, _ = oracle_port.jacobian(m, sol, qw2, curl2, pk, True)
+    assert_csr_equal(plan.row_ptr, plan.col_idx, vals2, oracle_matrix(oracle_port, I2, J2, V2, E, False))
+
+
+def test_explicit_signs_are_honoured(oracle_port):
+    """Signs that differ from the Mesh.m rule are stored and applied as given."""
+    mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, 3, 8)
+    flipped = sign.copy()
+    flipped[::5] *= -1
+    m2 = mex_inputs(mesh.P, mesh.T, t2e, flipped, tags)
+    pk = material.pack_material_data(synth.standard_materials())
+    qw, val, curl = quadrature.reference_data(2)
+    I, J, V, Ri, Rv = oracle_port.jacobian(m2, sol, qw, curl, pk, True)
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, flipped)
+    assert plan.info.signs_derived == 0
+    plan.set_materials(pk)
+    vals, res = plan.jacobian(dev(sol))
+    assert_csr_equal(plan.row_ptr, plan.col_idx, vals, oracle_matrix(oracle_port, I, J, V, E, False))
+    assert bits_equal(host(res), oracle_port.sparse_vec(Ri, Rv, E))
+
+
+def test_deterministic_repeat(oracle_port):
+    mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, 10, 4)
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
+    plan.set_materials(material.pack_material_data(synth.standard_materials()))
+    s = dev(sol)
+    v1, r1 = plan.jacobian(s)
+    v2, r2 = plan.jacobian(s)
+    assert torch.equal(v1.view(torch.int64), v2.view(torch.int64))
+    assert torch.equal(r1.view(torch.int64), r2.view(torch.int64))
+
+
+# ---- analytic properties ----------------------------------------------------------------
+
+def test_gradient_null_space_and_symmetry(oracle_port):
+    """A = grad(phi) (edge differences of a nodal field) has zero curl: R = 0, K A = 0."""
+    mesh, tags, edges, t2e, sign, m, E, _ = _nonlinear_case(oracle_port, 8, 6)
+    phi = np.random.default_rng(2).normal(size=mesh.num_nodes)
+    a = phi[edges[:, 1]] - phi[edges[:, 0]]
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
+    nu = np.where(tags == synth.IRON, material.NU0 / 1000, material.NU0)
+    k = plan.stiffness(dev(nu))
+    A = torch.sparse_csr_tensor(plan.row_ptr, plan.col_idx.long(), k, size=(E, E))
+    ka = A @ dev(a)
+    scale = torch.sparse_csr_tensor(plan.row_ptr, plan.col_idx.long(), k.abs(), size=(E, E)) @ dev(np.abs(a))
+    assert float((ka.abs() / scale.clamp_min(1e-300)).max()) < 1e-9
+    plan.set_materials(material.pack_material_data(synth.standard_materials()))
+    _, r = plan.jacobian(dev(a), calc_j=False)
+    assert float(r.abs().max()) < 1e-9 * float(scale.max())
+    # K is symmetric bit for bit for linear materials
+    Kd = A.to_dense()
+    assert torch.equal(Kd, Kd.T)
+
+
+def test_jacobian_matches_finite_differences(oracle_port):
+    mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, 5, 9, scale=0.05)
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
+    plan.set_materials(material.pack_material_data(synth.standard_materials()))
+    x = dev(sol)
+    vals, _ = plan.jacobian(x)
+    Jm = torch.sparse_csr_tensor(plan.row_ptr, plan.col_idx.long(), vals, size=(E, E))
+    d = dev(np.random.default_rng(1).normal(size=E)) * 1e-3 * x.abs().mean()
+    eps = 1e-3
+    _, rp = plan.jacobian(x + eps * d, calc_j=False)
+    _, rm = plan.jacobian(x - eps * d, calc_j=False)
+    fd = (rp - rm) / (2 * eps)
+    jd = Jm @ d
+    assert float((fd - jd).norm() / jd.norm()) < 1e-5
+
+
+# ---- errors are reported, not dereferenced ------------------------------------------------
+
+def test_errors_are_reported(oracle_port):
+    mesh = synth.kuhn_box(2, seed=0)
+    tags = synth.cube_layout(mesh)
+    edges, t2e, sign = oracle_port.generate_edges(mesh.T)
+    E = edges.shape[0]
+    bad = tags.copy()
+    bad[3] = 0
+    with pytest.raises(_lib.MagError) as ei:
+        AssemblyPlan(mesh.P, mesh.T, t2e, E, bad, sign)
+    assert ei.value.code == -2
+    flat = mesh.P.copy()
+    flat[mesh.T[0, 3]] = flat[mesh.T[0, 0]]  # collapse an element
+    with pytest.raises(_lib.MagError) as ei:
+        AssemblyPlan(flat, mesh.T, t2e, E, tags, sign)
+    assert ei.value.code in (-3, -2)
+    dofs = t2e.copy()
+    dofs[0, 0] = E + 5
+    with pytest.raises(_lib.MagError):
+        AssemblyPlan(mesh.P, mesh.T, dofs, E, tags, sign)
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
+    with pytest.raises(_lib.MagError):  # materials not set
+        plan.jacobian(dev(np.zeros(E)))
+    plan.set_materials(material.pack_material_data({1: material.create_linear(1.0)}))
+    with pytest.raises(_lib.MagError) as ei:  # tags 2, 3 have no entry
+        plan.jacobian(dev(np.zeros(E)))
+    assert ei.value.code == -2
