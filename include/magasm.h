@@ -168,6 +168,31 @@ int mag_mex_mass(const double *P, int64_t Nn, const double *T, int64_t Ne, const
                  const double *Signs, const double *Coeffs, int64_t ncoeffs, const double *Qw,
                  int nq, const double *ValRef, double *I, double *J, double *V);
 
+/* Allocation-free form of mag_mex_jacobian, for callers that cannot allocate
+ * device memory: a MEX function working on mxGPUArray buffers owned by
+ * MATLAB's allocator, a host inside another runtime's memory pool or under a
+ * fixed budget, or a path where cudaMalloc must not run. (No counterpart in
+ * the reference, whose MEX kernels run on the host.)
+ * The caller owns everything: d_* are device arrays in the reference's MEX
+ * layout (P [3*Nn], T [4*Ne] and Dofs/Signs [6*Ne] as doubles, 1-based;
+ * Tags [Ne]; SolA [Ndof]); outputs d_I/d_J/d_V [36*Ne] (untouched when
+ * calc_j == 0) and d_Ridx/d_Rval [6*Ne] on the device. Qw, CurlRef and the
+ * material tables are host arrays, as in mag_mex_jacobian. The element blocks
+ * go to a static device array inside the library (Ne <= 32768, nmat <= 64,
+ * nbrk <= 4096, ncoe <= 16384; larger sizes return MAG_E_UNSUPPORTED), which
+ * every GPU that loads the library holds until exit. The first call on a
+ * device looks up that array's address, so make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised. Synchronises `stream` to report index errors. */
+int mag_mex_jacobian_noalloc(const double *d_P, int64_t Nn, const double *d_T, int64_t Ne,
+                             const double *d_Dofs, const double *d_Signs, const double *d_Tags,
+                             const double *d_SolA, int64_t Ndof, const double *Qw, int nq,
+                             const double *CurlRef, const double *lin, const double *isNon,
+                             const double *maxB, int nmat, const double *brk, int nbrk,
+                             const double *coe, int ncoe, const double *start, const double *cnt,
+                             const double *coeStart, int calc_j, double *d_I, double *d_J,
+                             double *d_V, double *d_Ridx, double *d_Rval, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -56,6 +56,9 @@ _PROTOS = {
                           _dp], _int),
     "mag_mex_curl_curl": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _int, _dp, _dp, _dp, _dp], _int),
     "mag_mex_mass": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _i64, _dp, _int, _dp, _dp, _dp, _dp], _int),
+    "mag_mex_jacobian_noalloc": ([_vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _dp, _int, _dp, _dp,
+                                  _dp, _dp, _int, _dp, _int, _dp, _int, _dp, _dp, _dp, _int, _vp, _vp,
+                                  _vp, _vp, _vp, _vp], _int),
 }
 
 _LIB = None
