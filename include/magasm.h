@@ -51,9 +51,17 @@ typedef struct {
     int32_t max_row_nnz;
     int32_t wide_positions; /* 1 if some row exceeds 31 entries */
     int32_t signs_derived;  /* 1 if signs equal the Mesh.m:134 rule and are not stored */
-    int32_t reserved;
+    int32_t schedule;       /* MAG_SCHEDULE_* used by the Jacobian assembly */
+    int32_t fused_ring_tiles; /* element tiles the L2 scratch ring holds (MAG_SCHEDULE_L2_RING) */
+    int32_t fused_grid;     /* co-resident CTAs of that launch */
     int64_t device_bytes;   /* memory held by the handle */
 } mag_mesh_info;
+
+/* Jacobian assembly schedules; all give identical bits. */
+#define MAG_OPTION_SCHEDULE 1
+#define MAG_SCHEDULE_TWO_PASS 0   /* element kernel + row reduction through an HBM scratch slab */
+#define MAG_SCHEDULE_L2_RING 1    /* one persistent launch, scratch ring sized to stay in L2 */
+#define MAG_SCHEDULE_ROW_BLOCKS 2 /* one launch, no scratch: per-row element recompute (default) */
 
 /* ---- library ------------------------------------------------------------ */
 
@@ -85,6 +93,11 @@ int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t N
                     int64_t num_dofs, mag_mesh **out, void *stream);
 int mag_mesh_destroy(mag_mesh *mesh);
 int mag_mesh_get_info(const mag_mesh *mesh, mag_mesh_info *info);
+/* Handle options (MAG_OPTION_*). */
+int mag_mesh_set_option(mag_mesh *mesh, int option, int64_t value);
+/* Synchronise `stream` and report whether the last assemblies completed: MAG_E_TIMEOUT
+ * if a bounded device-side wait of the L2-ring schedule gave up. */
+int mag_mesh_check(mag_mesh *mesh, void *stream);
 /* Copy the structural pattern out (device buffers: row_ptr [num_dofs+1], col_idx [nnz]). */
 int mag_mesh_pattern(const mag_mesh *mesh, int64_t *d_row_ptr, int32_t *d_col_idx, void *stream);
 

@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmagasm.so")
 
 MAG_OK = 0
+SCHEDULE_TWO_PASS, SCHEDULE_L2_RING, SCHEDULE_ROW_BLOCKS = 0, 1, 2
 _ERRNAMES = {-1: "MAG_E_ARG", -2: "MAG_E_RANGE", -3: "MAG_E_GEOMETRY", -4: "MAG_E_CUDA",
              -5: "MAG_E_TIMEOUT", -6: "MAG_E_NOMEM", -7: "MAG_E_UNSUPPORTED"}
 
@@ -26,8 +27,8 @@ class MagError(RuntimeError):
 class MeshInfo(C.Structure):
     _fields_ = [("num_nodes", C.c_int64), ("num_elements", C.c_int64), ("num_dofs", C.c_int64),
                 ("nnz", C.c_int64), ("num_incidences", C.c_int64), ("max_row_nnz", C.c_int32),
-                ("wide_positions", C.c_int32), ("signs_derived", C.c_int32),
-                ("reserved", C.c_int32), ("device_bytes", C.c_int64)]
+                ("wide_positions", C.c_int32), ("signs_derived", C.c_int32), ("schedule", C.c_int32),
+                ("fused_ring_tiles", C.c_int32), ("fused_grid", C.c_int32), ("device_bytes", C.c_int64)]
 
 
 _vp = C.c_void_p
@@ -43,6 +44,8 @@ _PROTOS = {
     "mag_mesh_destroy": ([_vp], _int),
     "mag_mesh_get_info": ([_vp, C.POINTER(MeshInfo)], _int),
     "mag_mesh_pattern": ([_vp, _vp, _vp, _vp], _int),
+    "mag_mesh_set_option": ([_vp, _int, _i64], _int),
+    "mag_mesh_check": ([_vp, _vp], _int),
     "mag_mesh_set_quadrature": ([_vp, _dp, _int, _dp, _dp], _int),
     "mag_mesh_set_materials": ([_vp, _dp, _dp, _dp, _int, _dp, _int, _dp, _int, _dp, _dp, _dp], _int),
     "mag_assemble_jacobian": ([_vp, _vp, _vp, _vp, _int, _vp], _int),

@@ -6,6 +6,8 @@
 
 #include "assemble.cuh"
 #include "common.cuh"
+#include "fused.cuh"
+#include "rowblock.cuh"
 #include "internal.h"
 
 namespace mag {
@@ -299,6 +301,9 @@ struct mag_mesh {
     double *d_ref = nullptr;
     MaterialStore mat;
     int has_mat = 0;
+    FusedPlan fused;
+    RowBlockPlan rowblock;
+    int schedule = MAG_SCHEDULE_ROW_BLOCKS;
     int64_t bytes = 0;
 
     ElemData elems() const { return ElemData{xyz, tet, dofs, tags, signbits, ne}; }
@@ -315,6 +320,8 @@ void destroy_mesh(mag_mesh *m) {
     for (void *p : ptrs)
         if (p) cudaFree(p);
     free_pattern(&m->pat, nullptr);
+    free_fused_plan(&m->fused);
+    free_rowblock_plan(&m->rowblock);
     cudaDeviceSynchronize();
     delete m;
 }
@@ -439,6 +446,20 @@ int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t N
         return fail(MAG_E_NOMEM);
     }
     m->bytes += (int64_t)Ne * kScratchPerElem * 8;
+    // optional schedules; the two-pass kernels always work
+    if (build_rowblock_plan(m->rows(), &m->rowblock, s) == MAG_OK) {
+        m->bytes += m->rowblock.bytes;
+    } else {
+        free_rowblock_plan(&m->rowblock);
+        cudaGetLastError();
+    }
+    if (build_fused_plan(m->elems(), m->rows(), m->pat.max_row, &m->fused, s) == MAG_OK) {
+        m->bytes += m->fused.bytes;
+    } else {
+        free_fused_plan(&m->fused);
+        cudaGetLastError();
+    }
+    m->schedule = m->rowblock.ok ? MAG_SCHEDULE_ROW_BLOCKS : MAG_SCHEDULE_TWO_PASS;
     double qw[4], curl[72], val[72];
     default_reference_data(qw, curl, val);
     rc = make_quad(qw, 4, curl, val, &m->qp, &m->d_ref, s);
@@ -466,6 +487,9 @@ int mag_mesh_get_info(const mag_mesh *m, mag_mesh_info *info) {
     info->max_row_nnz = m->pat.max_row;
     info->wide_positions = m->pat.wide;
     info->signs_derived = m->signbits ? 0 : 1;
+    info->schedule = m->schedule;
+    info->fused_ring_tiles = m->fused.ring_tiles;
+    info->fused_grid = m->fused.grid;
     info->device_bytes = m->bytes;
     return MAG_OK;
 }
@@ -512,6 +536,16 @@ int mag_assemble_jacobian(mag_mesh *m, const double *d_sol, double *d_vals, doub
         return MAG_E_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
+    if (m->schedule == MAG_SCHEDULE_ROW_BLOCKS) {
+        MAG_TRY(launch_rowblock_jacobian(m->rowblock, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp, calc_j,
+                                         calc_j ? d_vals : nullptr, d_res, s));
+        return finish(s);
+    }
+    if (m->schedule == MAG_SCHEDULE_L2_RING) {
+        MAG_TRY(launch_fused_jacobian(m->fused, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp, calc_j,
+                                      calc_j ? d_vals : nullptr, d_res, s));
+        return finish(s);
+    }
     MAG_TRY(launch_jacobian_elems(m->elems(), d_sol, m->qp, m->mat.mp, calc_j, m->scratch, s));
     MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, calc_j ? d_vals : nullptr, d_res, s));
     return finish(s);
@@ -566,6 +600,36 @@ int mag_element_b(mag_mesh *m, const double *d_sol, double *d_b, double *d_bsq, 
     cudaStream_t s = (cudaStream_t)stream;
     MAG_TRY(launch_element_b(m->elems(), d_sol, d_b, d_bsq, s));
     return finish(s);
+}
+
+int mag_mesh_set_option(mag_mesh *m, int option, int64_t value) {
+    if (!m) {
+        set_error("null mesh handle");
+        return MAG_E_ARG;
+    }
+    if (option == MAG_OPTION_SCHEDULE) {
+        if ((value == MAG_SCHEDULE_L2_RING && !m->fused.ok) ||
+            (value == MAG_SCHEDULE_ROW_BLOCKS && !m->rowblock.ok) || value < 0 || value > 2) {
+            set_error("assembly schedule %lld is not available for this mesh", (long long)value);
+            return MAG_E_UNSUPPORTED;
+        }
+        m->schedule = (int)value;
+        return MAG_OK;
+    }
+    set_error("unknown option %d", option);
+    return MAG_E_ARG;
+}
+
+int mag_mesh_check(mag_mesh *m, void *stream) {
+    if (!m) {
+        set_error("null mesh handle");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_TRY(fused_status(m->fused, s));
+    MAG_CUDA_TRY(cudaStreamSynchronize(s));
+    MAG_CUDA_TRY(cudaGetLastError());
+    return MAG_OK;
 }
 
 int mag_csr_drop_zeros(const int64_t *d_row_ptr, const int32_t *d_col_idx, const double *d_vals,

@@ -71,6 +71,17 @@ class AssemblyPlan:
         self._keep = a
         self._materials_key = key
 
+    def set_schedule(self, schedule: int):
+        """Jacobian schedule: _lib.SCHEDULE_TWO_PASS, SCHEDULE_L2_RING or SCHEDULE_ROW_BLOCKS."""
+        _lib.check(self._lib.mag_mesh_set_option(self._h, 1, int(schedule)))
+        info = _lib.MeshInfo()
+        _lib.check(self._lib.mag_mesh_get_info(self._h, C.byref(info)))
+        self.info = info
+
+    def check(self, stream=None):
+        """Synchronise and raise if a bounded device-side wait gave up."""
+        _lib.check(self._lib.mag_mesh_check(self._h, _lib.stream_ptr(stream)))
+
     # ---- pattern -----------------------------------------------------------
     def _pattern(self):
         if self._row_ptr is None:

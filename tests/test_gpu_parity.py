@@ -347,3 +347,42 @@ def test_errors_are_reported(oracle_port):
     with pytest.raises(_lib.MagError) as ei:  # tags 2, 3 have no entry
         plan.jacobian(dev(np.zeros(E)))
     assert ei.value.code == -2
+
+
+# ---- the three Jacobian schedules ------------------------------------------------------------
+
+SCHEDULES = (_lib.SCHEDULE_ROW_BLOCKS, _lib.SCHEDULE_L2_RING, _lib.SCHEDULE_TWO_PASS)
+
+
+@pytest.mark.parametrize("n,seed", [(13, 21), (30, 22)])
+def test_schedules_agree_bit_for_bit(oracle_port, n, seed):
+    """Row blocks (default), the persistent L2-ring launch (ring reused many times at 30^3)
+    and the two-pass kernels give the same bits as each other and as the oracle, with and
+    without the Jacobian, on the fast and the general quadrature path."""
+    mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, n, seed)
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
+    assert plan.info.schedule == _lib.SCHEDULE_ROW_BLOCKS
+    if n >= 30:
+        assert 2 * plan.info.fused_ring_tiles < (mesh.num_elements + 255) // 256
+    pk = material.pack_material_data(synth.standard_materials())
+    plan.set_materials(pk)
+    x = dev(sol)
+    qw, val, curl = quadrature.reference_data(2)
+    qw2 = np.array([0.05, 0.04, 0.045, 0.0316666])
+    refs = {}
+    for name, w in (("std", qw), ("general", qw2)):
+        I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, w, curl, pk, True)
+        _, _, _, Ri0, Rv0 = oracle_port.jacobian(m, sol, w, curl, pk, False)
+        refs[name] = (oracle_matrix(oracle_port, I, J, V, E, False), oracle_port.sparse_vec(Ri, Rv, E),
+                      oracle_port.sparse_vec(Ri0, Rv0, E))
+    for name, w in (("std", qw), ("general", qw2)):
+        plan.set_quadrature(w, curl, val)
+        mat, vec, vec0 = refs[name]
+        for sch in SCHEDULES:
+            plan.set_schedule(sch)
+            v, r = plan.jacobian(x)
+            _, r0 = plan.jacobian(x, calc_j=False)
+            plan.check()
+            assert_csr_equal(plan.row_ptr, plan.col_idx, v, mat)
+            assert bits_equal(host(r), vec), (name, sch)
+            assert bits_equal(host(r0), vec0), (name, sch)
