@@ -153,6 +153,29 @@ int mag_csr_drop_zeros(const int64_t *d_row_ptr, const int32_t *d_col_idx, const
                        int64_t nrows, int64_t *d_row_ptr_out, int32_t *d_col_out,
                        double *d_vals_out, int64_t *nnz_out, void *stream);
 
+/* ---- batched complex frequency-domain assembly ------------------------------ */
+
+typedef struct mag_batch mag_batch;
+
+/* A_i = K_i(nu_i) + j*omega_i*M_i(sigma_i) for n independent meshes, the system
+ * FrequencySolver.solve forms (src/solver/FrequencySolver.m:87,125,131) without
+ * its regularisation term, assembled in ONE persistent launch over a work queue
+ * of (mesh, row block) items. d_nu[i] and d_sigma[i] are per-element device
+ * arrays (d_sigma[i] may be NULL: sigma = 1); d_vals[i] receives complex128
+ * values (re, im interleaved) on mesh i's structural pattern; omega in rad/s.
+ * Creation times every compiled variant (incidences per CTA x CTAs per SM) on
+ * these inputs, keeps the fastest, and captures its launch in a CUDA graph. */
+int mag_batch_create(mag_mesh *const *meshes, int n, const double *const *d_nu,
+                     const double *const *d_sigma, const double *omega, double *const *d_vals,
+                     mag_batch **out, void *stream);
+/* Replays the captured graph on `stream`. */
+int mag_batch_assemble(mag_batch *batch, void *stream);
+/* The chosen variant, its description, and the time (ms) each variant took
+ * during creation (times[] must hold mag_batch_variants() entries). */
+int mag_batch_variants(void);
+int mag_batch_tuning(const mag_batch *batch, int *chosen, double *times_ms, char *name, int name_len);
+int mag_batch_destroy(mag_batch *batch);
+
 /* ---- MEX-compatible entry points (host buffers, reference layout) --------- */
 
 /* [I,J,V,R_idx,R_val] = assemble_jacobian_kernel_mex(P,T,Dofs,Signs,Tags,SolA,

@@ -53,6 +53,11 @@ _PROTOS = {
     "mag_assemble_mass": ([_vp, _vp, _vp, _vp], _int),
     "mag_assemble_source": ([_vp, _vp, _vp, _vp], _int),
     "mag_element_b": ([_vp, _vp, _vp, _vp, _vp], _int),
+    "mag_batch_create": ([_vp, _int, _vp, _vp, _dp, _vp, C.POINTER(_vp), _vp], _int),
+    "mag_batch_assemble": ([_vp, _vp], _int),
+    "mag_batch_variants": ([], _int),
+    "mag_batch_tuning": ([_vp, C.POINTER(_int), _dp, C.c_char_p, _int], _int),
+    "mag_batch_destroy": ([_vp], _int),
     "mag_csr_drop_zeros": ([_vp, _vp, _vp, _i64, _vp, _vp, _vp, C.POINTER(_i64), _vp], _int),
     "mag_mex_jacobian": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _i64, _dp, _int, _dp, _dp, _dp,
                           _dp, _int, _dp, _int, _dp, _int, _dp, _dp, _dp, _int, _dp, _dp, _dp, _dp,

@@ -5,6 +5,7 @@
 #include <new>
 
 #include "assemble.cuh"
+#include "batch.cuh"
 #include "common.cuh"
 #include "fused.cuh"
 #include "rowblock.cuh"
@@ -637,6 +638,151 @@ int mag_csr_drop_zeros(const int64_t *d_row_ptr, const int32_t *d_col_idx, const
                        int64_t *nnz_out, void *stream) {
     return csr_drop_zeros(d_row_ptr, d_col_idx, d_vals, nrows, d_row_ptr_out, d_col_out, d_vals_out,
                           nnz_out, (cudaStream_t)stream);
+}
+
+// ---- batched complex assembly -----------------------------------------------------
+
+}  // extern "C"
+
+struct mag_batch {
+    BatchState st;
+    int chosen = 0;
+    double times[8] = {0};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+void destroy_batch(mag_batch *b) {
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    batch_free_variants(&b->st);
+    for (int32_t *p : b->st.owned)
+        if (p) cudaFree(p);
+    delete b;
+}
+}  // namespace
+
+extern "C" {
+
+int mag_batch_variants(void) { return batch_num_variants(); }
+
+int mag_batch_create(mag_mesh *const *meshes, int n, const double *const *d_nu, const double *const *d_sigma,
+                     const double *omega, double *const *d_vals, mag_batch **out, void *stream) {
+    if (!meshes || n < 1 || !d_nu || !omega || !d_vals || !out) {
+        set_error("mag_batch_create: bad arguments");
+        return MAG_E_ARG;
+    }
+    *out = nullptr;
+    cudaStream_t s = (cudaStream_t)stream;
+    mag_batch *b = new (std::nothrow) mag_batch();
+    if (!b) return MAG_E_NOMEM;
+    auto fail = [&](int rc) {
+        destroy_batch(b);
+        return rc;
+    };
+    for (int i = 0; i < n; i++) {
+        mag_mesh *m = meshes[i];
+        if (!m || !d_nu[i] || !d_vals[i] || !m->rowblock.ok || !m->qp.standard_curl) {
+            set_error("mag_batch_create: mesh %d is missing, has no row-block plan, or uses a "
+                      "non-standard curl table", i);
+            return fail(MAG_E_ARG);
+        }
+        BatchInstance bi{};
+        bi.m = m->elems();
+        bi.rp = m->rows();
+        bi.nu = d_nu[i];
+        bi.sigma = d_sigma ? d_sigma[i] : nullptr;
+        bi.val_ref = m->qp.val_ref;
+        bi.nq = m->qp.nq;
+        for (int q = 0; q < m->qp.nq; q++) bi.qw[q] = m->qp.qw[q];
+        bi.nq4 = (m->qp.nq == 4 && m->qp.uniform_w) ? 1 : 0;
+        bi.omega = omega[i];
+        bi.vals = d_vals[i];
+        b->st.inst_host.push_back(bi);
+        b->st.inst_ne.push_back(m->ne);
+        b->st.block_row256.push_back(m->rowblock.block_row);
+        b->st.nblocks256.push_back(m->rowblock.nblocks);
+        RowBlockPlan p128;
+        int rc = build_rowblock_plan(m->rows(), &p128, s, 128);
+        if (rc != MAG_OK) return fail(rc);
+        b->st.owned.push_back(p128.block_row);
+        b->st.block_row128.push_back(p128.block_row);
+        b->st.nblocks128.push_back(p128.nblocks);
+    }
+    int rc = batch_build(&b->st, s);
+    if (rc != MAG_OK) return fail(rc);
+    // autotune: time every variant on these inputs, keep the fastest
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return fail(MAG_E_CUDA);
+    double best = 1e300;
+    for (int v = 0; v < batch_num_variants(); v++) {
+        rc = batch_launch(b->st, v, s);  // warm-up
+        if (rc != MAG_OK) break;
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3; r++) batch_launch(b->st, v, s);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = MAG_E_CUDA;
+            break;
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        b->times[v] = ms / 3.0;
+        if (b->times[v] < best) {
+            best = b->times[v];
+            b->chosen = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != MAG_OK) return fail(rc);
+    // capture the chosen launch (capture needs a stream other than the legacy default)
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return fail(MAG_E_CUDA);
+    cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+        batch_launch(b->st, b->chosen, cs);
+        ce = cudaStreamEndCapture(cs, &b->graph);
+    }
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    cudaStreamDestroy(cs);
+    if (ce != cudaSuccess) {
+        set_error("mag_batch_create: graph capture failed: %s", cudaGetErrorString(ce));
+        return fail(MAG_E_CUDA);
+    }
+    *out = b;
+    return MAG_OK;
+}
+
+int mag_batch_assemble(mag_batch *b, void *stream) {
+    if (!b || !b->exec) {
+        set_error("mag_batch_assemble: bad handle");
+        return MAG_E_ARG;
+    }
+    MAG_CUDA_TRY(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+    return MAG_OK;
+}
+
+int mag_batch_tuning(const mag_batch *b, int *chosen, double *times_ms, char *name, int name_len) {
+    if (!b) {
+        set_error("mag_batch_tuning: bad handle");
+        return MAG_E_ARG;
+    }
+    if (chosen) *chosen = b->chosen;
+    if (times_ms)
+        for (int v = 0; v < batch_num_variants(); v++) times_ms[v] = b->times[v];
+    if (name && name_len > 0) {
+        std::strncpy(name, batch_variant_name(b->chosen), name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    return MAG_OK;
+}
+
+int mag_batch_destroy(mag_batch *b) {
+    destroy_batch(b);
+    return MAG_OK;
 }
 
 // ---- MEX-compatible entry points ------------------------------------------------

@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(kBlockInc, 4) k_rowblock(RBArgs A) {
 
 }  // namespace
 
-int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s) {
+int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc) {
     *out = RowBlockPlan{};
     std::vector<int32_t> ip((size_t)rp.ndof + 1);
     MAG_CUDA_TRY(cudaMemcpyAsync(ip.data(), rp.inc_ptr, ip.size() * 4, cudaMemcpyDeviceToHost, s));
@@ -203,12 +203,12 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s) {
     while (a < rp.ndof) {
         starts.push_back((int32_t)a);
         int64_t b = a + 1;
-        if (ip[b] - ip[a] > kBlockInc) {
+        if (ip[b] - ip[a] > block_inc) {
             set_error("row-block plan: row %lld has %d incidences (at most %d)", (long long)a,
-                      ip[b] - ip[a], kBlockInc);
+                      ip[b] - ip[a], block_inc);
             return MAG_E_UNSUPPORTED;
         }
-        while (b < rp.ndof && ip[b + 1] - ip[a] <= kBlockInc && b - a < kBlockInc) b++;
+        while (b < rp.ndof && ip[b + 1] - ip[a] <= block_inc && b - a < block_inc) b++;
         a = b;
     }
     starts.push_back((int32_t)rp.ndof);

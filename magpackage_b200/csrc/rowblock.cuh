@@ -18,7 +18,7 @@ struct RowBlockPlan {
     int ok = 0;
 };
 
-int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s);
+int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc = kBlockInc);
 void free_rowblock_plan(RowBlockPlan *p);
 int launch_rowblock_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *sol,
                              const QuadParams &qp, const MaterialParams &mp, int calcj, double *vals,

@@ -182,3 +182,53 @@ def generate_edges(T):
     _lib.check(L.mag_generate_edges(_ptr(T), ne, nn, _ptr(edges), _ptr(t2e), _ptr(sign), C.byref(E),
                                     _lib.stream_ptr()))
     return edges[: E.value], t2e, sign
+
+
+class ComplexBatch:
+    """K_i(nu_i) + j*omega_i*M_i(sigma_i) for many meshes in one graph-captured launch.
+
+    plans: AssemblyPlan per mesh; nus / sigmas: per-element CUDA float64 tensors
+    (a sigma may be None: sigma = 1); omegas: rad/s. ``values[i]`` holds mesh i's
+    complex128 CSR values on its structural pattern after ``assemble()``.
+    """
+
+    def __init__(self, plans, nus, sigmas, omegas, stream=None):
+        self._lib = _lib.lib()
+        n = len(plans)
+        self.plans = list(plans)
+        self.nus = [t.contiguous() for t in nus]
+        self.sigmas = [None if t is None else t.contiguous() for t in sigmas]
+        self.values = [torch.empty(p.nnz, dtype=torch.complex128, device="cuda") for p in plans]
+        H = (C.c_void_p * n)(*[p._h.value for p in plans])
+        NU = (C.c_void_p * n)(*[t.data_ptr() for t in self.nus])
+        SG = (C.c_void_p * n)(*[0 if t is None else t.data_ptr() for t in self.sigmas])
+        VA = (C.c_void_p * n)(*[t.data_ptr() for t in self.values])
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        h = C.c_void_p()
+        _lib.check(self._lib.mag_batch_create(H, n, NU, SG, _lib.dptr(om), VA, C.byref(h),
+                                              _lib.stream_ptr(stream)))
+        self._h = h
+        self.omegas = om
+
+    def assemble(self, stream=None):
+        _lib.check(self._lib.mag_batch_assemble(self._h, _lib.stream_ptr(stream)))
+        return self.values
+
+    def tuning(self):
+        nv = self._lib.mag_batch_variants()
+        chosen = C.c_int()
+        times = np.zeros(nv)
+        name = C.create_string_buffer(128)
+        _lib.check(self._lib.mag_batch_tuning(self._h, C.byref(chosen), _lib.dptr(times), name, 128))
+        return chosen.value, times, name.value.decode()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mag_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

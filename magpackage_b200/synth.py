@@ -144,3 +144,25 @@ def standard_materials(iron_nonlinear: bool = True):
 
 
 SIGMA_AL = 3.526e7
+
+
+def frequency_sweep_instances(count: int = 64, n_min: int = 8, n_max: int = 48, f_min: float = 10.0,
+                              f_max: float = 1e4, seed: int = 0):
+    """Independent jittered cubes of uneven size for the batched complex workload.
+
+    Instance k has n_k = round(n_min + (n_max - n_min) k / (count - 1)) hexahedra per
+    side (6 tetrahedra each), its own seeded jitter and region boxes, and frequency
+    f_k = f_min * (f_max / f_min)^(k / (count - 1)). Yields (mesh, tags, nu, sigma, omega).
+    """
+    from .material import NU0
+
+    rng = np.random.default_rng(seed)
+    for k in range(count):
+        t = k / max(count - 1, 1)
+        n = int(round(n_min + (n_max - n_min) * t))
+        mesh = kuhn_box(n, seed=seed * 1000 + k)
+        tags = random_box_layout(mesh, rng)
+        nu = np.where(tags == IRON, NU0 / 1000.0, NU0)
+        sigma = np.where(tags == ALUMINIUM, SIGMA_AL, 0.0)
+        omega = 2.0 * np.pi * f_min * (f_max / f_min) ** t
+        yield mesh, tags, nu, sigma, omega
