@@ -176,6 +176,38 @@ int mag_batch_variants(void);
 int mag_batch_tuning(const mag_batch *batch, int *chosen, double *times_ms, char *name, int name_len);
 int mag_batch_destroy(mag_batch *batch);
 
+/* ---- per-element reluctivity predictor (no counterpart in the reference) ---- */
+
+/* A 4 -> 64 -> 64 -> 64 -> 1 SiLU MLP whose hidden GEMMs run on the 5th-generation
+ * tensor cores (BF16 operands, FP32 accumulation in tensor memory) with FP32
+ * master weights and Adam. It predicts log-reluctivity per element from the
+ * previous steps' |B|, the source and the material, to seed the first Jacobian
+ * of a Newton solve through the per-element nu entry (mag_assemble_stiffness,
+ * the Assembler.assembleStiffness(space, nu_vec) path, src/Assembler.m:26-39).
+ * Parameters: W1[64][4] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4. */
+typedef struct mag_mlp mag_mlp;
+int mag_mlp_num_params(void);
+int mag_mlp_create(const float *init_params, mag_mlp **out);
+int mag_mlp_destroy(mag_mlp *mlp);
+int mag_mlp_get_params(const mag_mlp *mlp, float *host_params);
+int mag_mlp_set_params(mag_mlp *mlp, const float *host_params);
+/* y[rows] = f(feats[rows][4]); z[rows][3][64] (pre-activations) may be NULL. */
+int mag_mlp_forward(mag_mlp *mlp, const float *d_feats, int64_t rows, float *d_y, float *d_z, void *stream);
+/* nu = clamp(exp(y * y_scale + y_shift), nu_min, nu_max) written to d_nu[d_rows[i]]
+ * (d_rows NULL: d_nu[i]). */
+int mag_mlp_predict_nu(mag_mlp *mlp, const float *d_feats, int64_t rows, const int32_t *d_rows,
+                       double y_scale, double y_shift, double nu_min, double nu_max, double *d_nu,
+                       void *stream);
+/* Forward + backward of L = sum_i loss_scale/2 * (y_i - target_i)^2: d_grad[num_params]
+ * (NULL: internal buffer), summed over rows in a fixed order. d_y [rows], d_z [rows][3][64]. */
+int mag_mlp_gradient(mag_mlp *mlp, const float *d_feats, const float *d_target, int64_t rows,
+                     float loss_scale, float *d_y, float *d_z, float *d_grad, void *stream);
+/* One Adam step (lr, betas 0.9/0.999) on the mean-squared error of a minibatch. */
+int mag_mlp_train_step(mag_mlp *mlp, const float *d_feats, const float *d_target, int64_t rows,
+                       float lr, float *d_y, float *d_z, void *stream);
+/* Synchronise; MAG_E_TIMEOUT if a tensor-core completion wait gave up. */
+int mag_mlp_check(mag_mlp *mlp, void *stream);
+
 /* ---- MEX-compatible entry points (host buffers, reference layout) --------- */
 
 /* [I,J,V,R_idx,R_val] = assemble_jacobian_kernel_mex(P,T,Dofs,Signs,Tags,SolA,

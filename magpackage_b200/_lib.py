@@ -58,6 +58,17 @@ _PROTOS = {
     "mag_batch_variants": ([], _int),
     "mag_batch_tuning": ([_vp, C.POINTER(_int), _dp, C.c_char_p, _int], _int),
     "mag_batch_destroy": ([_vp], _int),
+    "mag_mlp_num_params": ([], _int),
+    "mag_mlp_create": ([C.POINTER(C.c_float), C.POINTER(_vp)], _int),
+    "mag_mlp_destroy": ([_vp], _int),
+    "mag_mlp_get_params": ([_vp, C.POINTER(C.c_float)], _int),
+    "mag_mlp_set_params": ([_vp, C.POINTER(C.c_float)], _int),
+    "mag_mlp_forward": ([_vp, _vp, _i64, _vp, _vp, _vp], _int),
+    "mag_mlp_predict_nu": ([_vp, _vp, _i64, _vp, C.c_double, C.c_double, C.c_double, C.c_double, _vp, _vp],
+                           _int),
+    "mag_mlp_gradient": ([_vp, _vp, _vp, _i64, C.c_float, _vp, _vp, _vp, _vp], _int),
+    "mag_mlp_train_step": ([_vp, _vp, _vp, _i64, C.c_float, _vp, _vp, _vp], _int),
+    "mag_mlp_check": ([_vp, _vp], _int),
     "mag_csr_drop_zeros": ([_vp, _vp, _vp, _i64, _vp, _vp, _vp, C.POINTER(_i64), _vp], _int),
     "mag_mex_jacobian": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _i64, _dp, _int, _dp, _dp, _dp,
                           _dp, _int, _dp, _int, _dp, _int, _dp, _dp, _dp, _int, _dp, _dp, _dp, _dp,

@@ -10,6 +10,7 @@
 #include "fused.cuh"
 #include "rowblock.cuh"
 #include "internal.h"
+#include "mlp.cuh"
 
 namespace mag {
 
@@ -782,6 +783,144 @@ int mag_batch_tuning(const mag_batch *b, int *chosen, double *times_ms, char *na
 
 int mag_batch_destroy(mag_batch *b) {
     destroy_batch(b);
+    return MAG_OK;
+}
+
+// ---- reluctivity predictor MLP --------------------------------------------------------
+
+}  // extern "C"
+
+struct mag_mlp {
+    float *params = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr, *partial = nullptr;
+    __nv_bfloat16 *ops = nullptr;
+    int *err = nullptr;
+    int grid = 0, step = 0;
+};
+
+namespace {
+void destroy_mlp(mag_mlp *n) {
+    if (!n) return;
+    void *p[] = {n->params, n->grad, n->m, n->v, n->partial, n->ops, n->err};
+    for (void *q : p)
+        if (q) cudaFree(q);
+    delete n;
+}
+int mlp_grid(int64_t n, int cap) {
+    int64_t tiles = (n + 127) / 128;
+    return (int)(tiles < cap ? (tiles < 1 ? 1 : tiles) : cap);
+}
+}  // namespace
+
+extern "C" {
+
+int mag_mlp_num_params(void) { return kMlpParams; }
+
+int mag_mlp_create(const float *init_params, mag_mlp **out) {
+    if (!init_params || !out) {
+        set_error("mag_mlp_create: bad arguments");
+        return MAG_E_ARG;
+    }
+    *out = nullptr;
+    mag_mlp *n = new (std::nothrow) mag_mlp();
+    if (!n) return MAG_E_NOMEM;
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    n->grid = 2 * (nsm > 0 ? nsm : 1);
+    size_t pb = (size_t)kMlpParams * sizeof(float);
+    if (cudaMalloc(&n->params, pb) != cudaSuccess || cudaMalloc(&n->grad, pb) != cudaSuccess ||
+        cudaMalloc(&n->m, pb) != cudaSuccess || cudaMalloc(&n->v, pb) != cudaSuccess ||
+        cudaMalloc(&n->partial, pb * n->grid) != cudaSuccess ||
+        cudaMalloc(&n->ops, (size_t)kMlpOperandElems * sizeof(__nv_bfloat16)) != cudaSuccess ||
+        cudaMalloc(&n->err, sizeof(int)) != cudaSuccess) {
+        destroy_mlp(n);
+        set_error("mag_mlp_create: out of device memory");
+        return MAG_E_NOMEM;
+    }
+    cudaMemcpy(n->params, init_params, pb, cudaMemcpyHostToDevice);
+    cudaMemset(n->m, 0, pb);
+    cudaMemset(n->v, 0, pb);
+    cudaMemset(n->err, 0, sizeof(int));
+    if (mlp_pack(n->params, n->ops, nullptr) != MAG_OK || cudaDeviceSynchronize() != cudaSuccess) {
+        destroy_mlp(n);
+        set_error("mag_mlp_create: CUDA error");
+        return MAG_E_CUDA;
+    }
+    *out = n;
+    return MAG_OK;
+}
+
+int mag_mlp_destroy(mag_mlp *n) {
+    destroy_mlp(n);
+    return MAG_OK;
+}
+
+int mag_mlp_get_params(const mag_mlp *n, float *host) {
+    if (!n || !host) return MAG_E_ARG;
+    MAG_CUDA_TRY(cudaMemcpy(host, n->params, (size_t)kMlpParams * sizeof(float), cudaMemcpyDeviceToHost));
+    return MAG_OK;
+}
+
+int mag_mlp_set_params(mag_mlp *n, const float *host) {
+    if (!n || !host) return MAG_E_ARG;
+    MAG_CUDA_TRY(cudaMemcpy(n->params, host, (size_t)kMlpParams * sizeof(float), cudaMemcpyHostToDevice));
+    MAG_TRY(mlp_pack(n->params, n->ops, nullptr));
+    MAG_CUDA_TRY(cudaDeviceSynchronize());
+    return MAG_OK;
+}
+
+int mag_mlp_forward(mag_mlp *n, const float *d_feats, int64_t rows, float *d_y, float *d_z, void *stream) {
+    if (!n || !d_feats || rows <= 0 || !d_y) {
+        set_error("mag_mlp_forward: bad arguments");
+        return MAG_E_ARG;
+    }
+    MlpForwardArgs a{d_feats, rows, n->params, n->ops, d_y, d_z, nullptr, nullptr, 0, 0, 0, 0, n->err};
+    return mlp_forward(a, mlp_grid(rows, 4 * n->grid), (cudaStream_t)stream);
+}
+
+int mag_mlp_predict_nu(mag_mlp *n, const float *d_feats, int64_t rows, const int32_t *d_rows, double y_scale,
+                       double y_shift, double nu_min, double nu_max, double *d_nu, void *stream) {
+    if (!n || !d_feats || rows <= 0 || !d_nu || !(nu_min > 0) || !(nu_max >= nu_min)) {
+        set_error("mag_mlp_predict_nu: bad arguments");
+        return MAG_E_ARG;
+    }
+    MlpForwardArgs a{d_feats, rows, n->params, n->ops, nullptr, nullptr, d_nu, d_rows, y_scale, y_shift,
+                     nu_min, nu_max, n->err};
+    return mlp_forward(a, mlp_grid(rows, 4 * n->grid), (cudaStream_t)stream);
+}
+
+int mag_mlp_gradient(mag_mlp *n, const float *d_feats, const float *d_target, int64_t rows, float loss_scale,
+                     float *d_y, float *d_z, float *d_grad, void *stream) {
+    if (!n || !d_feats || !d_target || rows <= 0 || !d_y || !d_z) {
+        set_error("mag_mlp_gradient: bad arguments");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MlpForwardArgs fa{d_feats, rows, n->params, n->ops, d_y, d_z, nullptr, nullptr, 0, 0, 0, 0, n->err};
+    MAG_TRY(mlp_forward(fa, mlp_grid(rows, 4 * n->grid), s));
+    MlpBackwardArgs ba{d_feats, d_z, d_y, d_target, rows, loss_scale, n->params, n->ops, n->partial,
+                       d_grad ? d_grad : n->grad, n->err};
+    return mlp_backward(ba, mlp_grid(rows, n->grid), s);
+}
+
+int mag_mlp_train_step(mag_mlp *n, const float *d_feats, const float *d_target, int64_t rows, float lr,
+                       float *d_y, float *d_z, void *stream) {
+    MAG_TRY(mag_mlp_gradient(n, d_feats, d_target, rows, 2.0f / (float)rows, d_y, d_z, nullptr, stream));
+    cudaStream_t s = (cudaStream_t)stream;
+    n->step++;
+    MAG_TRY(mlp_adam(n->params, n->grad, n->m, n->v, lr, 0.9f, 0.999f, 1e-8f, n->step, s));
+    return mlp_pack(n->params, n->ops, s);
+}
+
+int mag_mlp_check(mag_mlp *n, void *stream) {
+    if (!n) return MAG_E_ARG;
+    int h = 0;
+    MAG_CUDA_TRY(cudaMemcpyAsync(&h, n->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    MAG_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    if (h) {
+        set_error("an MLP kernel's bounded wait on its tensor-core completion gave up");
+        return MAG_E_TIMEOUT;
+    }
     return MAG_OK;
 }
 

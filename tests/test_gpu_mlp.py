@@ -1,0 +1,65 @@
+"""Tensor-core MLP kernels against the CPU oracle (oracle/mlp_ref.py)."""
+import numpy as np
+import pytest
+import torch
+
+from magpackage_b200.mlp import MLP, init_params
+from oracle import mlp_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(n, seed):
+    rng = np.random.default_rng(seed)
+    p = init_params(seed)
+    p[256:320] = rng.normal(0, 0.1, 64)  # nonzero biases exercise every path
+    x = rng.normal(0, 1, (n, 4)).astype(np.float32)
+    t = rng.normal(0, 1, n).astype(np.float32)
+    return p, x, t
+
+
+@pytest.mark.parametrize("n", [128, 300, 4096])
+def test_forward_matches_oracle(n):
+    p, x, _ = _case(n, 1)
+    net = MLP(p)
+    y, _ = net.forward(torch.as_tensor(x, device="cuda"))
+    net.check()
+    y_ref, _ = mlp_ref.forward(p, x)
+    y = y.cpu().numpy()
+    # FP32 accumulation order differs from the float64 oracle; BF16 rounding points match
+    assert np.max(np.abs(y - y_ref)) <= 2e-3 * (1 + np.max(np.abs(y_ref)))
+    assert np.corrcoef(y, y_ref)[0, 1] > 0.99999
+
+
+@pytest.mark.parametrize("n", [256, 1000])
+def test_gradient_matches_oracle(n):
+    p, x, t = _case(n, 2)
+    net = MLP(p)
+    y, g = net.gradient(torch.as_tensor(x, device="cuda"), torch.as_tensor(t, device="cuda"), 2.0 / n)
+    net.check()
+    y_ref, g_ref = mlp_ref.gradient(p, x, t, 2.0 / n)
+    g = g.cpu().numpy()
+    rel = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    assert rel < 1e-2, rel
+    # every parameter block individually
+    for a, b in ((0, 256), (256, 320), (320, 4416), (4416, 4480), (4480, 8576), (8576, 8640), (8640, 8704)):
+        r = np.linalg.norm(g[a:b] - g_ref[a:b]) / max(np.linalg.norm(g_ref[a:b]), 1e-12)
+        assert r < 2e-2, (a, b, r)
+
+
+def test_training_reduces_loss():
+    rng = np.random.default_rng(3)
+    n = 16384
+    x = rng.normal(0, 1, (n, 4)).astype(np.float32)
+    t = (np.tanh(x[:, 0]) + 0.5 * x[:, 1] * x[:, 2] - 0.3 * x[:, 3]).astype(np.float32)
+    net = MLP(init_params(3))
+    xd, td = torch.as_tensor(x, device="cuda"), torch.as_tensor(t, device="cuda")
+    y0, _ = net.forward(xd)
+    l0 = float(((y0 - td) ** 2).mean())
+    for ep in range(30):
+        for i in range(0, n, 4096):
+            net.train_step(xd[i:i + 4096].contiguous(), td[i:i + 4096].contiguous(), 3e-3)
+    net.check()
+    y1, _ = net.forward(xd)
+    l1 = float(((y1 - td) ** 2).mean())
+    assert l1 < 0.1 * l0, (l0, l1)
