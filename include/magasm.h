@@ -131,6 +131,22 @@ int mag_assemble_jacobian(mag_mesh *mesh, const double *d_sol, double *d_vals, d
  * (assemble_curl_curl_kernel_mex.cpp:18-121 + Assembler.m:37-38). */
 int mag_assemble_stiffness(mag_mesh *mesh, const double *d_nu, double *d_vals, void *stream);
 
+/* Newton residual at d_sol with the tangent evaluated at a seeded state: per
+ * element the flux density B of d_sol scaled by d_bscale[e] (the learned warm
+ * start's first Jacobian; no counterpart in the reference). Same outputs as
+ * mag_assemble_jacobian with calc_j = 1; d_bscale = 1 everywhere reproduces it
+ * to rounding. Standard curl table only. */
+int mag_assemble_jacobian_seeded(mag_mesh *mesh, const double *d_sol, const double *d_bscale,
+                                 double *d_vals, double *d_res, void *stream);
+
+/* Per-element scale of the seeded tangent: beta_e = (|B_e| + |B_hat_e|)/(2|B_e|),
+ * B_e the flux density of d_sol and |B_hat_e|^2 where the element's nonlinear
+ * nu(|B|^2) equals d_nu_hat[e] (a predicted reluctivity), i.e. the tangent at the
+ * midpoint between the current and the predicted state. beta = 1 for linear
+ * materials, d_nu_hat[e] <= 0 or B_e = 0. No counterpart in the reference. */
+int mag_seed_midpoint(mag_mesh *mesh, const double *d_sol, const double *d_nu_hat, double *d_bscale,
+                      void *stream);
+
 /* Sigma-weighted Nedelec mass M(sigma) (assemble_mass_kernel_mex.cpp:17-127 +
  * Assembler.m:52-53,71-72). d_sigma [Ne], or NULL for sigma = 1 (the
  * reference's empty Coeffs, assemble_mass_kernel_mex.cpp:155,187). */
@@ -207,6 +223,48 @@ int mag_mlp_train_step(mag_mlp *mlp, const float *d_feats, const float *d_target
                        float lr, float *d_y, float *d_z, void *stream);
 /* Synchronise; MAG_E_TIMEOUT if a tensor-core completion wait gave up. */
 int mag_mlp_check(mag_mlp *mlp, void *stream);
+
+/* ---- sparse algebra for the Newton driver ------------------------------------
+ * CSR arguments: d_row_ptr [n+1] int64, d_col_idx [nnz] int32, d_vals [nnz]. */
+
+/* y = A x (the products of TransientSolver.m:289-300). */
+int mag_csr_spmv(int64_t n, const int64_t *d_row_ptr, const int32_t *d_col_idx, const double *d_vals,
+                 const double *d_x, double *d_y, void *stream);
+
+/* Dirichlet elimination in place: A <- M_free A M_free + M_fixed and
+ * rhs[fixed] = 0 (BoundaryCondition.applyDirichlet, src/BoundaryCondition.m:81-112).
+ * d_fixed [n] is nonzero for a fixed dof; d_rhs may be NULL. Entries that
+ * become zero stay in the pattern (MATLAB's result would not store them). */
+int mag_csr_apply_dirichlet(int64_t n, const int64_t *d_row_ptr, const int32_t *d_col_idx, double *d_vals,
+                            const uint8_t *d_fixed, double *d_rhs, void *stream);
+
+/* Preconditioned conjugate gradients, the stand-in for the reference's MUMPS
+ * solve (LinearSolver.solve, src/solver/LinearSolver.m:22-46), for symmetric
+ * positive definite A. d_x holds the initial guess and receives the solution;
+ * stops when ||b - A x|| <= rtol ||b|| (recursive residual) or after max_iter
+ * iterations. Jacobi preconditioner, plus the auxiliary gradient space when set.
+ * Deterministic (fixed-order reductions). Outputs: iterations, ||r||/||b||,
+ * status 1 converged / 2 iteration limit / 3 breakdown (returns MAG_E_GEOMETRY).
+ * Synchronises the host once per 32 iterations. */
+typedef struct mag_pcg mag_pcg;
+int mag_pcg_create(int64_t n, mag_pcg **out);
+int mag_pcg_destroy(mag_pcg *pcg);
+/* Optional auxiliary gradient space for the preconditioner:
+ * z = D^-1 r + G (dn_inv .* (G^T r)), with G [n x ni] the discrete gradient
+ * (edge-node incidence, +-1) restricted to free edges and interior nodes, given
+ * both as G and as G^T in CSR, and dn_inv = 1 / diag(G^T A G). The arrays stay
+ * owned by the caller and must outlive the solves. ni = 0 removes it. */
+int mag_pcg_set_aux(mag_pcg *pcg, int64_t ni, const int64_t *d_g_row_ptr, const int32_t *d_g_col_idx,
+                    const double *d_g_vals, const int64_t *d_gt_row_ptr, const int32_t *d_gt_col_idx,
+                    const double *d_gt_vals, const double *d_dn_inv);
+int mag_pcg_solve(mag_pcg *pcg, const int64_t *d_row_ptr, const int32_t *d_col_idx, const double *d_vals,
+                  const double *d_b, double *d_x, double rtol, int max_iter, int *iters, double *relres,
+                  int *status, void *stream);
+
+/* Per-element reluctivity nu(|B|^2) and d nu / d|B|^2 at the solution d_sol
+ * (the values the Jacobian kernel evaluates, MexMaterialUtils.hpp:24-87);
+ * needs mag_mesh_set_materials. Either output may be NULL. */
+int mag_element_nu(mag_mesh *mesh, const double *d_sol, double *d_nu, double *d_dnu, void *stream);
 
 /* ---- MEX-compatible entry points (host buffers, reference layout) --------- */
 

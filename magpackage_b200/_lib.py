@@ -53,6 +53,16 @@ _PROTOS = {
     "mag_assemble_mass": ([_vp, _vp, _vp, _vp], _int),
     "mag_assemble_source": ([_vp, _vp, _vp, _vp], _int),
     "mag_element_b": ([_vp, _vp, _vp, _vp, _vp], _int),
+    "mag_element_nu": ([_vp, _vp, _vp, _vp, _vp], _int),
+    "mag_assemble_jacobian_seeded": ([_vp, _vp, _vp, _vp, _vp, _vp], _int),
+    "mag_seed_midpoint": ([_vp, _vp, _vp, _vp, _vp], _int),
+    "mag_csr_spmv": ([_i64, _vp, _vp, _vp, _vp, _vp, _vp], _int),
+    "mag_csr_apply_dirichlet": ([_i64, _vp, _vp, _vp, _vp, _vp, _vp], _int),
+    "mag_pcg_create": ([_i64, C.POINTER(_vp)], _int),
+    "mag_pcg_destroy": ([_vp], _int),
+    "mag_pcg_set_aux": ([_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _int),
+    "mag_pcg_solve": ([_vp, _vp, _vp, _vp, _vp, _vp, C.c_double, _int, C.POINTER(_int), _dp, C.POINTER(_int),
+                       _vp], _int),
     "mag_batch_create": ([_vp, _int, _vp, _vp, _dp, _vp, C.POINTER(_vp), _vp], _int),
     "mag_batch_assemble": ([_vp, _vp], _int),
     "mag_batch_variants": ([], _int),

@@ -60,6 +60,114 @@ __global__ void __launch_bounds__(128) k_jacobian_elems(ElemData m, const double
     }
 }
 
+// ---- phase 1: Newton block with a seeded tangent ---------------------------
+// Residual at the element's state B (as k_jacobian_elems); tangent evaluated at the
+// seeded state beta_e * B: nu(|beta B|^2) Ci.Cj + 2 nu'(|beta B|^2) (beta B.Ci)(beta B.Cj).
+// Standard curl table only (constant curls, so one evaluation per element).
+__global__ void __launch_bounds__(128) k_jacobian_seeded_elems(ElemData m, const double *__restrict__ sol,
+                                                               const double *__restrict__ bscale, QuadParams qp,
+                                                               MaterialParams mp, double *__restrict__ scratch) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    int4 t = m.tet[e];
+    int d[6];
+    load_dofs(m.dofs, e, d);
+    unsigned sb = m.signbits ? m.signbits[e] : derived_signs(t);
+    int tag = m.tags[e];
+    Geo g;
+    geometry(m.xyz, t, g);
+    double a[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) a[i] = d[i] >= 0 ? flip(__ldg(sol + d[i]), (sb >> i) & 1) : 0.0;
+    double C[6][3];
+    curls_standard(g, C);
+    double B[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        double v = a[0] * C[0][c];
+#pragma unroll
+        for (int i = 1; i < 6; i++) v = v + a[i] * C[i][c];
+        B[c] = v;
+    }
+    double w[kMaxQuad];
+    for (int q = 0; q < qp.nq; q++) w[q] = qp.qw[q] * g.adet;
+    double nu, dnu, num, dnum;
+    material_eval(mp, tag, dot3(B, B), nu, dnu);
+    const double be = bscale[e];
+    material_eval(mp, tag, (be * be) * dot3(B, B), num, dnum);
+    double b[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) b[i] = dot3(B, C[i]);
+    double *dst = scratch + e * kScratchPerElem;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        double row[6];
+        const double gi = 2.0 * dnum * (be * b[i]);
+#pragma unroll
+        for (int j = 0; j < 6; j++)
+            row[j] = flip(qsum(num * dot3(C[i], C[j]) + gi * (be * b[j]), w, qp.nq, qp.uniform_w),
+                          ((sb >> i) ^ (sb >> j)) & 1);
+        store_row(dst + i * kScratchStride, row, flip(qsum(nu * b[i], w, qp.nq, qp.uniform_w), (sb >> i) & 1));
+    }
+}
+
+// Midpoint seed of the tangent: beta_e = (|B_e| + |B_hat_e|) / (2 |B_e|), |B_hat_e|^2 the
+// point where the element's nonlinear nu(|B|^2) equals the predicted nu_hat_e (bisection;
+// nu is nondecreasing in |B|^2 for the B-H tables used). beta = 1 for linear materials,
+// nu_hat <= 0, or B = 0.
+__global__ void __launch_bounds__(128) k_seed_midpoint(ElemData m, const double *__restrict__ sol,
+                                                       const double *__restrict__ nu_hat, MaterialParams mp,
+                                                       double *__restrict__ bscale) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    const int tag = m.tags[e];
+    const double target = nu_hat[e];
+    double beta = 1.0;
+    if (target > 0.0 && __ldg(mp.is_non + tag - 1) != 0.0) {
+        int4 t = m.tet[e];
+        int d[6];
+        load_dofs(m.dofs, e, d);
+        unsigned sb = m.signbits ? m.signbits[e] : derived_signs(t);
+        Geo g;
+        geometry(m.xyz, t, g);
+        double C[6][3];
+        curls_standard(g, C);
+        double a[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) a[i] = d[i] >= 0 ? flip(__ldg(sol + d[i]), (sb >> i) & 1) : 0.0;
+        double B[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double v = a[0] * C[0][c];
+#pragma unroll
+            for (int i = 1; i < 6; i++) v = v + a[i] * C[i][c];
+            B[c] = v;
+        }
+        const double bp = sqrt(dot3(B, B));
+        if (bp > 0.0) {
+            double lo = 0.0, hi = 4.0 * __ldg(mp.max_bsq + tag - 1), nu, dnu;
+            material_eval(mp, tag, hi, nu, dnu);
+            double s_hat = hi;
+            if (target < nu) {
+                material_eval(mp, tag, 0.0, nu, dnu);
+                if (target <= nu) {
+                    s_hat = 0.0;
+                } else {
+                    for (int it = 0; it < 64; it++) {
+                        double mid = 0.5 * (lo + hi);
+                        material_eval(mp, tag, mid, nu, dnu);
+                        if (nu < target) lo = mid;
+                        else hi = mid;
+                    }
+                    s_hat = 0.5 * (lo + hi);
+                }
+            }
+            beta = 0.5 * (bp + sqrt(s_hat)) / bp;
+        }
+    }
+    bscale[e] = beta;
+}
+
 // ---- phase 1: curl-curl K(nu) ----------------------------------------------
 
 template <bool STDCURL>
@@ -197,7 +305,9 @@ __global__ void __launch_bounds__(128) k_source_elems(ElemData m, const double *
 // ---- element B (post-processing / predictor features) -------------------------
 
 __global__ void __launch_bounds__(128) k_element_b(ElemData m, const double *__restrict__ sol,
-                                                   double *__restrict__ bout, double *__restrict__ bsq) {
+                                                   double *__restrict__ bout, double *__restrict__ bsq,
+                                                   MaterialParams mp, double *__restrict__ nu_out,
+                                                   double *__restrict__ dnu_out) {
     int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
     int4 t = m.tet[e];
@@ -225,6 +335,12 @@ __global__ void __launch_bounds__(128) k_element_b(ElemData m, const double *__r
         bout[3 * e + 2] = B[2];
     }
     if (bsq) bsq[e] = dot3(B, B);
+    if (nu_out || dnu_out) {  // the reluctivity the Jacobian kernel evaluates for this element
+        double nu, dnu;
+        material_eval(mp, m.tags[e], dot3(B, B), nu, dnu);
+        if (nu_out) nu_out[e] = nu;
+        if (dnu_out) dnu_out[e] = dnu;
+    }
 }
 
 // ---- phase 2: fixed-order row reduction --------------------------------------
@@ -323,6 +439,18 @@ int launch_jacobian_elems(const ElemData &m, const double *sol, const QuadParams
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
 
+int launch_jacobian_seeded_elems(const ElemData &m, const double *sol, const double *bscale, const QuadParams &qp,
+                                 const MaterialParams &mp, double *scratch, cudaStream_t s) {
+    k_jacobian_seeded_elems<<<blocks(m.ne, 128), 128, 0, s>>>(m, sol, bscale, qp, mp, scratch);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+int launch_seed_midpoint(const ElemData &m, const double *sol, const double *nu_hat, const MaterialParams &mp,
+                         double *bscale, cudaStream_t s) {
+    k_seed_midpoint<<<blocks(m.ne, 128), 128, 0, s>>>(m, sol, nu_hat, mp, bscale);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
 int launch_stiffness_elems(const ElemData &m, const double *nu, const QuadParams &qp,
                            double *scratch, cudaStream_t s) {
     unsigned g = blocks(m.ne, 128);
@@ -343,8 +471,11 @@ int launch_source_elems(const ElemData &m, const double *js, const QuadParams &q
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
 
-int launch_element_b(const ElemData &m, const double *sol, double *b, double *bsq, cudaStream_t s) {
-    k_element_b<<<blocks(m.ne, 128), 128, 0, s>>>(m, sol, b, bsq);
+int launch_element_b(const ElemData &m, const double *sol, double *b, double *bsq, cudaStream_t s,
+                     const MaterialParams *mp, double *nu, double *dnu) {
+    MaterialParams none{};
+    k_element_b<<<blocks(m.ne, 128), 128, 0, s>>>(m, sol, b, bsq, mp ? *mp : none, mp ? nu : nullptr,
+                                                  mp ? dnu : nullptr);
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
 

@@ -9,13 +9,18 @@ namespace mag {
 
 int launch_jacobian_elems(const ElemData &m, const double *sol, const QuadParams &qp,
                           const MaterialParams &mp, int calcj, double *scratch, cudaStream_t s);
+int launch_jacobian_seeded_elems(const ElemData &m, const double *sol, const double *bscale, const QuadParams &qp,
+                                 const MaterialParams &mp, double *scratch, cudaStream_t s);
+int launch_seed_midpoint(const ElemData &m, const double *sol, const double *nu_hat, const MaterialParams &mp,
+                         double *bscale, cudaStream_t s);
 int launch_stiffness_elems(const ElemData &m, const double *nu, const QuadParams &qp,
                            double *scratch, cudaStream_t s);
 int launch_mass_elems(const ElemData &m, const double *sigma, const QuadParams &qp, double *scratch,
                       cudaStream_t s);
 int launch_source_elems(const ElemData &m, const double *js, const QuadParams &qp, double *scratch,
                         cudaStream_t s);
-int launch_element_b(const ElemData &m, const double *sol, double *b, double *bsq, cudaStream_t s);
+int launch_element_b(const ElemData &m, const double *sol, double *b, double *bsq, cudaStream_t s,
+                     const MaterialParams *mp = nullptr, double *nu = nullptr, double *dnu = nullptr);
 int launch_rows_reduce(const RowPlan &rp, int max_row, const double *scratch, double *vals,
                        double *vec, cudaStream_t s);
 int launch_to_triplets(const double *scratch, const int32_t *dofs, int64_t ne, int calcj, double *I,

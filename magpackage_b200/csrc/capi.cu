@@ -11,6 +11,7 @@
 #include "rowblock.cuh"
 #include "internal.h"
 #include "mlp.cuh"
+#include "sparse.cuh"
 
 namespace mag {
 
@@ -565,6 +566,38 @@ int mag_assemble_stiffness(mag_mesh *m, const double *d_nu, double *d_vals, void
     return finish(s);
 }
 
+int mag_assemble_jacobian_seeded(mag_mesh *m, const double *d_sol, const double *d_bscale, double *d_vals,
+                                 double *d_res, void *stream) {
+    MAG_TRY(require_ready(m, true));
+    if (!d_sol || !d_bscale || !d_vals || !d_res) {
+        set_error("mag_assemble_jacobian_seeded: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (!m->qp.standard_curl) {
+        set_error("mag_assemble_jacobian_seeded: needs the standard Nedelec curl table");
+        return MAG_E_UNSUPPORTED;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_TRY(launch_jacobian_seeded_elems(m->elems(), d_sol, d_bscale, m->qp, m->mat.mp, m->scratch, s));
+    MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, d_vals, d_res, s));
+    return finish(s);
+}
+
+int mag_seed_midpoint(mag_mesh *m, const double *d_sol, const double *d_nu_hat, double *d_bscale, void *stream) {
+    MAG_TRY(require_ready(m, true));
+    if (!d_sol || !d_nu_hat || !d_bscale) {
+        set_error("mag_seed_midpoint: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (!m->qp.standard_curl) {
+        set_error("mag_seed_midpoint: needs the standard Nedelec curl table");
+        return MAG_E_UNSUPPORTED;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_TRY(launch_seed_midpoint(m->elems(), d_sol, d_nu_hat, m->mat.mp, d_bscale, s));
+    return finish(s);
+}
+
 int mag_assemble_mass(mag_mesh *m, const double *d_sigma, double *d_vals, void *stream) {
     MAG_TRY(require_ready(m, false));
     if (!d_vals) {
@@ -601,6 +634,21 @@ int mag_element_b(mag_mesh *m, const double *d_sol, double *d_b, double *d_bsq, 
     }
     cudaStream_t s = (cudaStream_t)stream;
     MAG_TRY(launch_element_b(m->elems(), d_sol, d_b, d_bsq, s));
+    return finish(s);
+}
+
+int mag_element_nu(mag_mesh *m, const double *d_sol, double *d_nu, double *d_dnu, void *stream) {
+    MAG_TRY(require_ready(m, true));
+    if (!d_sol || (!d_nu && !d_dnu)) {
+        set_error("mag_element_nu: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (!m->qp.standard_curl) {
+        set_error("mag_element_nu: needs the standard Nedelec curl table");
+        return MAG_E_UNSUPPORTED;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_TRY(launch_element_b(m->elems(), d_sol, nullptr, nullptr, s, &m->mat.mp, d_nu, d_dnu));
     return finish(s);
 }
 
@@ -922,6 +970,81 @@ int mag_mlp_check(mag_mlp *n, void *stream) {
         return MAG_E_TIMEOUT;
     }
     return MAG_OK;
+}
+
+// ---- sparse algebra ---------------------------------------------------------------
+
+int mag_csr_spmv(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, const double *x, double *y,
+                 void *stream) {
+    if (n <= 0 || !rp || !ci || !v || !x || !y) {
+        set_error("mag_csr_spmv: bad arguments");
+        return MAG_E_ARG;
+    }
+    MAG_TRY(csr_spmv(n, rp, ci, v, x, y, (cudaStream_t)stream));
+    return MAG_OK;
+}
+
+int mag_csr_apply_dirichlet(int64_t n, const int64_t *rp, const int32_t *ci, double *v, const uint8_t *fixed,
+                            double *rhs, void *stream) {
+    if (n <= 0 || !rp || !ci || !v || !fixed) {
+        set_error("mag_csr_apply_dirichlet: bad arguments");
+        return MAG_E_ARG;
+    }
+    MAG_TRY(csr_dirichlet(n, rp, ci, v, fixed, rhs, (cudaStream_t)stream));
+    return MAG_OK;
+}
+
+}  // extern "C"
+
+struct mag_pcg {
+    PcgSolver *s = nullptr;
+};
+
+extern "C" {
+
+int mag_pcg_create(int64_t n, mag_pcg **out) {
+    if (n <= 0 || !out) {
+        set_error("mag_pcg_create: bad arguments");
+        return MAG_E_ARG;
+    }
+    *out = nullptr;
+    mag_pcg *p = new (std::nothrow) mag_pcg();
+    if (!p) return MAG_E_NOMEM;
+    if (pcg_create(n, &p->s) != MAG_OK) {
+        delete p;
+        set_error("mag_pcg_create: out of device memory");
+        return MAG_E_NOMEM;
+    }
+    *out = p;
+    return MAG_OK;
+}
+
+int mag_pcg_destroy(mag_pcg *p) {
+    if (p) {
+        pcg_destroy(p->s);
+        delete p;
+    }
+    return MAG_OK;
+}
+
+int mag_pcg_set_aux(mag_pcg *p, int64_t ni, const int64_t *g_rp, const int32_t *g_ci, const double *g_v,
+                    const int64_t *gt_rp, const int32_t *gt_ci, const double *gt_v, const double *dn_inv) {
+    if (!p || ni < 0 || (ni > 0 && (!g_rp || !g_ci || !g_v || !gt_rp || !gt_ci || !gt_v || !dn_inv))) {
+        set_error("mag_pcg_set_aux: bad arguments");
+        return MAG_E_ARG;
+    }
+    int rc = pcg_set_aux(p->s, ni, g_rp, g_ci, g_v, gt_rp, gt_ci, gt_v, dn_inv);
+    if (rc != MAG_OK) set_error("mag_pcg_set_aux: out of device memory");
+    return rc;
+}
+
+int mag_pcg_solve(mag_pcg *p, const int64_t *rp, const int32_t *ci, const double *v, const double *b, double *x,
+                  double rtol, int max_iter, int *iters, double *relres, int *status, void *stream) {
+    if (!p || !rp || !ci || !v || !b || !x || !(rtol >= 0) || max_iter <= 0) {
+        set_error("mag_pcg_solve: bad arguments");
+        return MAG_E_ARG;
+    }
+    return pcg_solve(p->s, rp, ci, v, b, x, rtol, max_iter, iters, relres, status, (cudaStream_t)stream);
 }
 
 // ---- MEX-compatible entry points ------------------------------------------------

@@ -134,6 +134,68 @@ def ecore_layout(mesh: BoxMesh):
     return tags, coil & ~iron
 
 
+# Coil of the transient workload: a rectangular winding around the E-core's centre
+# leg. In the x-z plane it is the ring between the outer box [0.13,0.27]x[0.01,0.19]
+# and the window [0.17,0.23]x[0.05,0.15] (the window holds the leg with a gap);
+# along y it spans [0.12,0.28], its current fading linearly over the first and last
+# 0.02 m.
+COIL_OUTER = ((0.13, 0.27), (0.01, 0.19))
+COIL_WINDOW = ((0.17, 0.23), (0.05, 0.15))
+COIL_Y = (0.12, 0.28)
+COIL_RAMP = 0.02
+
+
+def ecore_coil_layout(mesh: BoxMesh) -> np.ndarray:
+    """Tags for the transient workload: E-core iron, ring coil around the centre leg, air."""
+    tags, _ = ecore_layout(mesh)
+    tags[tags == COIL] = AIR
+    c = mesh.centroids()
+    x, y, z = c[:, 0], c[:, 1], c[:, 2]
+    (ox0, ox1), (oz0, oz1) = COIL_OUTER
+    (wx0, wx1), (wz0, wz1) = COIL_WINDOW
+    outer = (x > ox0) & (x < ox1) & (z > oz0) & (z < oz1)
+    window = (x > wx0) & (x < wx1) & (z > wz0) & (z < wz1)
+    ring = outer & ~window & (y > COIL_Y[0]) & (y < COIL_Y[1])
+    tags[ring & (tags == AIR)] = COIL
+    return tags
+
+
+def _ring_phi(x, z):
+    """0 outside the ring's outer box, 1 in the window, linear across the 0.04 m wall."""
+    (ox0, ox1), (oz0, oz1) = COIL_OUTER
+    w = COIL_WINDOW[0][0] - ox0
+    d = np.minimum(np.minimum(x - ox0, ox1 - x), np.minimum(z - oz0, oz1 - z))
+    return np.clip(d / w, 0.0, 1.0), w
+
+
+def _ramp_integral(y):
+    """X(y) = integral from 0 to y of the coil's axial profile chi (0 -> 1 -> 0 along y)."""
+    y0, y1 = COIL_Y
+    r = COIL_RAMP
+    y = np.clip(np.asarray(y, dtype=np.float64), y0, y1)
+    up = np.minimum(y - y0, r)
+    X = up * up / (2 * r)                                   # rising ramp
+    X = X + np.clip(y - (y0 + r), 0.0, (y1 - r) - (y0 + r))  # plateau
+    down = np.clip(y - (y1 - r), 0.0, r)
+    return X + down - down * down / (2 * r)                 # falling ramp
+
+
+def coil_edge_values(P: np.ndarray, edges: np.ndarray) -> np.ndarray:
+    """Edge values t_e of a current vector potential T = w phi(x, z) chi(y) e_y.
+
+    J = curl T = w chi (-d phi/dz, 0, d phi/dx) has unit magnitude in the ring
+    walls (where chi = 1), circulates around the centre leg and vanishes in the
+    window. t_e = w phi(midpoint) (X(y_b) - X(y_a)) with X the antiderivative of
+    chi: on edges inside the window (phi = 1) that is the exact increment of a
+    potential, so the discrete current, the element curl of t, is exactly zero
+    there, and being a curl it is exactly divergence-free everywhere.
+    """
+    a, b = P[edges[:, 0]], P[edges[:, 1]]
+    mid = 0.5 * (a + b)
+    phi, w = _ring_phi(mid[:, 0], mid[:, 2])
+    return w * phi * (_ramp_integral(b[:, 1]) - _ramp_integral(a[:, 1]))
+
+
 def standard_materials(iron_nonlinear: bool = True):
     """Material map used by the workloads: air/aluminium/coil linear, iron Froehlich."""
     from .material import NU0, create_linear_nu, create_nonlinear, froehlich_bh

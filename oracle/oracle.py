@@ -116,6 +116,15 @@ class Port(_Lib):
                                  _d(Ri), _d(Rv))
         return I[:nK], J[:nK], V[:nK], Ri, Rv
 
+    def material_eval(self, bsq, tags, packed):
+        """(nu, dnu/d|B|^2) at |B|^2 = bsq for 1-based tags (MexMaterialUtils.hpp:24-87)."""
+        bsq, tags = _f64(bsq), _f64(tags)
+        pk = [_f64(a) for a in packed.as_tuple()]
+        nu, dnu = np.zeros(bsq.size), np.zeros(bsq.size)
+        self.lib.oracle_material_eval(_d(bsq), _d(tags), C.c_int64(bsq.size), *[_d(a) for a in pk], _d(nu),
+                                      _d(dnu))
+        return nu, dnu
+
     def curl_curl(self, m: MexInputs, nu, qw, curl):
         ne = m.ne
         I, J, V = (np.zeros(36 * ne) for _ in range(3))

@@ -117,6 +117,15 @@ static void material_eval(double s, int tag, const double *lin, const double *is
     *dnu_out = dnu;
 }
 
+void oracle_material_eval(const double *s, const double *Tags, int64_t n, const double *lin,
+                          const double *isNon, const double *maxB, const double *brk,
+                          const double *coe, const double *start, const double *cnt,
+                          const double *coeStart, double *nu, double *dnu) {
+    for (int64_t i = 0; i < n; i++)
+        material_eval(s[i], (int)Tags[i], lin, isNon, maxB, brk, coe, start, cnt, coeStart, nu + i,
+                      dnu + i);
+}
+
 void oracle_jacobian(const double *P, const double *T, int64_t Ne, const double *Dofs,
                      const double *Signs, const double *Tags, const double *SolA, const double *Qw,
                      int nq, const double *CurlRef, const double *lin, const double *isNon,

@@ -33,6 +33,13 @@ void oracle_jacobian(const double *P, const double *T, int64_t Ne, const double 
                      const double *cnt, const double *coeStart, int calcJ, double *I, double *J,
                      double *V, double *Ridx, double *Rval);
 
+/* evaluate_nu_derivative (MexMaterialUtils.hpp:24-87) at n values s = |B|^2 with
+ * 1-based tags; the packed tables as for oracle_jacobian. */
+void oracle_material_eval(const double *s, const double *Tags, int64_t n, const double *lin,
+                          const double *isNon, const double *maxB, const double *brk,
+                          const double *coe, const double *start, const double *cnt,
+                          const double *coeStart, double *nu, double *dnu);
+
 /* Curl-curl element kernel, src/mex/assemble_curl_curl_kernel_mex.cpp:18-121. */
 void oracle_curl_curl(const double *P, const double *T, int64_t Ne, const double *Dofs,
                       const double *Signs, const double *Nu, const double *Qw, int nq,
