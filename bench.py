@@ -41,7 +41,39 @@ WORKLOADS = {
     # name: (n, description)
     "jacobian_60": (60, "Newton Jacobian + residual, 60^3 Kuhn cube (1.296M tets), FP64"),
     "jacobian_110": (110, "Newton Jacobian + residual, 110^3 Kuhn cube (7.986M tets), FP64"),
+    "jacobian_110_mlp": (110, "Newton Jacobian + residual, 110^3 Kuhn cube (7.986M tets), FP64, plus BF16 "
+                              "MLP nu inference over all elements per Newton step"),
 }
+
+
+def run_transient(args):
+    """Config 4: E-core transient, plain vs learned warm start (Newton iterations per step at 1e-8)."""
+    import torch
+
+    from magpackage_b200.transient import TransientConfig, compare
+
+    torch.cuda.set_device(0)
+    cfg = TransientConfig()
+    t0 = time.perf_counter()
+    out = compare(cfg)
+    wall = time.perf_counter() - t0
+    p, l, i = out["plain"], out["learned"], out["ideal"]
+    steps = l["steps"]
+    line = {
+        "metric": "Newton iters/step learned vs plain @1e-8", "value": l["newton"] / steps,
+        "unit": "Newton iterations per step (learned warm start)", "n_gpus": 1, "steps": steps, "warmup": 0,
+        "higher_is_better": False, "scaling": "none", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "E-core transient 40x40x20 hexes x6 (192k tets), J = 2e6 sin(2 pi 50 t), "
+                               "backward Euler dt = 1e-4, 200 steps, Newton to ||R|| <= 1e-8 max(||F||, 1); "
+                               "MLP trained on steps 1-100, compared on 101-200", **out["config"]},
+        "plain": p, "learned": l, "ideal": i, "plain_first_half": out["plain_first"], "train": out["train"],
+        "per_step_newton": out["per_step"],
+        "ratio_learned_over_plain": {"newton": l["newton"] / p["newton"],
+                                     "assemblies": l["assemblies"] / p["assemblies"],
+                                     "gpu_ms": l["gpu_ms"] / p["gpu_ms"]},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
 
 
 def run_batched_complex(args):
@@ -228,7 +260,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="jacobian_60", choices=sorted(WORKLOADS) + ["batched_complex"])
+    ap.add_argument("--workload", default="jacobian_60",
+                    choices=sorted(WORKLOADS) + ["batched_complex", "transient"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--schedule", default="row-blocks", choices=["row-blocks", "l2-ring", "two-pass"],
                     help="Jacobian assembly schedule (all give identical bits)")
@@ -244,6 +277,9 @@ def main():
         return
     if args.workload == "batched_complex":
         run_batched_complex(args)
+        return
+    if args.workload == "transient":
+        run_transient(args)
         return
 
     import torch
@@ -275,8 +311,26 @@ def main():
     vals, res = plan.new_values(), plan.new_vector()
     stream = torch.cuda.current_stream()
 
+    with_mlp = args.workload.endswith("_mlp")
+    mlp = None
+    if with_mlp:
+        # per-element features |B|_{t-1}, |B|_{t-2}, |J|, material id, resident in HBM; the
+        # network predicts nu for every element each Newton step (config 5)
+        from magpackage_b200.mlp import MLP, init_params
+
+        mlp = MLP(init_params(1))
+        rows = torch.arange(ne, dtype=torch.int32, device="cuda")
+        feats = torch.randn((ne, 4), dtype=torch.float32, device="cuda", generator=torch.Generator(
+            device="cuda").manual_seed(rank))
+        nu_hat = torch.empty(ne, dtype=torch.float64, device="cuda")
+
+    def infer():
+        mlp.predict_nu(feats, rows, nu_hat, 0.5, 5.0, 1.0, 1e6)
+
     def step():
         plan.jacobian(sol, vals, res)
+        if with_mlp:
+            infer()
 
     for _ in range(args.warmup):
         step()
@@ -297,6 +351,22 @@ def main():
         dist.barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
     plan.check()  # raises if a bounded device-side wait gave up
+    ms_asm, ms_mlp = ms, 0.0
+    if with_mlp:
+        mlp.check()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            plan.jacobian(sol, vals, res)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms_asm = ev0.elapsed_time(ev1) / args.steps
+        ev0.record(stream)
+        for _ in range(args.steps):
+            infer()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms_mlp = ev0.elapsed_time(ev1) / args.steps
+        mlp.check()
 
     # e2e: host buffers through the C ABI, copies inside the timed region
     h_sol = torch.empty(E, dtype=torch.float64, pin_memory=True)
@@ -308,6 +378,8 @@ def main():
     def e2e_step():
         d_sol.copy_(h_sol, non_blocking=True)
         plan.jacobian(d_sol, vals, res)
+        if with_mlp:
+            infer()
         h_vals.copy_(vals, non_blocking=True)
         h_res.copy_(res, non_blocking=True)
 
@@ -342,7 +414,7 @@ def main():
     if rank == 0:
         b_elem = algorithmic_bytes_per_elem(ne, mesh.num_nodes, E, nnz)
         peak, peak_kind = measured_peak()
-        achieved = b_elem * ne / (ms * 1e-3) / 1e9
+        achieved = b_elem * ne / (ms_asm * 1e-3) / 1e9
         value = world * ne / (ms * 1e-3) / 1e6
         out = {
             "metric": "Jacobian assembly Melem/s (FP64 CSR)", "value": value, "unit": "Melem/s",
@@ -365,10 +437,13 @@ def main():
                                                       " (element kernel + row reduction)")},
             "e2e": {"value": world * ne / (e2e_ms * 1e-3) / 1e6, "unit": "Melem/s",
                     "h2d_bytes_per_step": 8 * E, "d2h_bytes_per_step": 8 * (nnz + E)},
-            "gpu_launches": (1 if single else 2) * args.steps,
+            "gpu_launches": ((1 if single else 2) + (1 if with_mlp else 0)) * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
         }
+        if with_mlp:
+            out["split_ms"] = {"assembly": ms_asm, "mlp_inference": ms_mlp,
+                               "mlp_gflops": 2 * ne * (4 * 64 + 64 * 64 * 2 + 64) / (ms_mlp * 1e-3) / 1e9}
         print(json.dumps(out), flush=True)
     plan.close()
     if dist:

@@ -427,7 +427,7 @@ def summarize(stats) -> dict:
     return out
 
 
-def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, epochs: int = 30,
+def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, epochs: int = 120,
             seed: int = 0, log=None, ideal: bool = True) -> dict:
     """Plain run over all steps; train on the first half; rerun the second half learned (and ideal)."""
     from .mlp import NuPredictor
