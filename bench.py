@@ -41,6 +41,8 @@ WORKLOADS = {
     # name: (n, description)
     "jacobian_60": (60, "Newton Jacobian + residual, 60^3 Kuhn cube (1.296M tets), FP64"),
     "jacobian_110": (110, "Newton Jacobian + residual, 110^3 Kuhn cube (7.986M tets), FP64"),
+    "jacobian_60_mlp": (60, "Newton Jacobian + residual, 60^3 Kuhn cube (1.296M tets), FP64, plus BF16 MLP nu "
+                            "inference over all elements per Newton step"),
     "jacobian_110_mlp": (110, "Newton Jacobian + residual, 110^3 Kuhn cube (7.986M tets), FP64, plus BF16 "
                               "MLP nu inference over all elements per Newton step"),
 }
