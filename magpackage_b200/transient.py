@@ -422,6 +422,7 @@ def summarize(stats) -> dict:
     out["max_res_over_tol"] = float(max(s.res / s.tol_abs for s in stats))
     errs = [s.nu_rel_err for s in stats if s.nu_rel_err == s.nu_rel_err]
     out["nu_rel_err_mean"] = float(np.mean(errs)) if errs else None
+    out["nu_rel_err_median"] = float(np.median(errs)) if errs else None
     errs = [s.nu_rel_err_max for s in stats if s.nu_rel_err_max == s.nu_rel_err_max]
     out["nu_rel_err_max"] = float(np.max(errs)) if errs else None
     return out
@@ -456,6 +457,8 @@ def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, 
         xs = dict(plain.x)
         x_half = xs[half]
         b_hist = (plain.bmag[half - 1], plain.bmag[half - 2] if half >= 2 else zero)
+        # the second half again without a seed, after warm-up, for a like-for-like device time
+        plain2 = run(prob, half + 1, cfg.steps, x_half, b_hist, "plain")
         learned = run(prob, half + 1, cfg.steps, x_half, b_hist, "learned", pred)
         ideal_rec = run(prob, half + 1, cfg.steps, x_half, b_hist, "ideal", reference_x=xs) if ideal else None
         out = {
@@ -464,12 +467,12 @@ def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, 
                        "dt": cfg.dt, "train_steps": half, "tol": cfg.tol, "reg": prob.reg,
                        "sigma_iron": cfg.sigma_iron},
             "plain_first": summarize(plain.stats[:half]),
-            "plain": summarize(plain.stats[half:]),
+            "plain": summarize(plain2.stats),
             "learned": summarize(learned.stats),
             "ideal": summarize(ideal_rec.stats) if ideal else None,
             "train": {"samples": int(feats.shape[0]), "epochs": epochs, "loss_first": hist[0],
                       "loss_last": hist[-1], "gpu_ms": train_ms},
-            "per_step": {"plain": [s.newton for s in plain.stats[half:]],
+            "per_step": {"plain": [s.newton for s in plain2.stats],
                          "learned": [s.newton for s in learned.stats],
                          "ideal": [s.newton for s in ideal_rec.stats] if ideal else None},
         }
