@@ -265,7 +265,8 @@ def main():
     ap.add_argument("--workload", default="jacobian_60",
                     choices=sorted(WORKLOADS) + ["batched_complex", "transient"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--schedule", default="row-blocks", choices=["row-blocks", "l2-ring", "two-pass"],
+    ap.add_argument("--schedule", default="shared-row-blocks",
+                    choices=["shared-row-blocks", "row-blocks", "l2-ring", "two-pass"],
                     help="Jacobian assembly schedule (all give identical bits)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -304,7 +305,8 @@ def main():
     E = int(edges.shape[0])
     plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
     plan.set_materials(packed)
-    sched_id = {"row-blocks": _lib.SCHEDULE_ROW_BLOCKS, "l2-ring": _lib.SCHEDULE_L2_RING,
+    sched_id = {"shared-row-blocks": _lib.SCHEDULE_SHARED_ROW_BLOCKS,
+                "row-blocks": _lib.SCHEDULE_ROW_BLOCKS, "l2-ring": _lib.SCHEDULE_L2_RING,
                 "two-pass": _lib.SCHEDULE_TWO_PASS}[args.schedule]
     plan.set_schedule(sched_id)
     single = sched_id != _lib.SCHEDULE_TWO_PASS
@@ -426,7 +428,10 @@ def main():
             "config": {"workload": desc, "elements": ne, "edges": E, "nnz": nnz,
                        "l2": "inputs larger than L2 (per-step working set > 700 MB)",
                        "parallelism": f"{world} independent instance(s)",
-                       "schedule": {_lib.SCHEDULE_ROW_BLOCKS: "row blocks: one launch, per-row element "
+                       "schedule": {_lib.SCHEDULE_SHARED_ROW_BLOCKS: "row blocks: one launch, no scratch, "
+                                                                     "each block's distinct elements "
+                                                                     "evaluated once in shared memory",
+                                    _lib.SCHEDULE_ROW_BLOCKS: "row blocks: one launch, per-row element "
                                                               "recompute, no scratch",
                                     _lib.SCHEDULE_L2_RING: "one persistent launch, L2 scratch ring of "
                                                            f"{plan.info.fused_ring_tiles} tiles",

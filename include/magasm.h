@@ -61,7 +61,9 @@ typedef struct {
 #define MAG_OPTION_SCHEDULE 1
 #define MAG_SCHEDULE_TWO_PASS 0   /* element kernel + row reduction through an HBM scratch slab */
 #define MAG_SCHEDULE_L2_RING 1    /* one persistent launch, scratch ring sized to stay in L2 */
-#define MAG_SCHEDULE_ROW_BLOCKS 2 /* one launch, no scratch: per-row element recompute (default) */
+#define MAG_SCHEDULE_ROW_BLOCKS 2 /* one launch, no scratch: per-row element recompute */
+#define MAG_SCHEDULE_SHARED_ROW_BLOCKS 3 /* as 2, each block's distinct elements evaluated once in shared
+                                            memory (default; standard curl table, else runs as 2) */
 
 /* ---- library ------------------------------------------------------------ */
 

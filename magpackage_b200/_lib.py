@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmagasm.so")
 
 MAG_OK = 0
-SCHEDULE_TWO_PASS, SCHEDULE_L2_RING, SCHEDULE_ROW_BLOCKS = 0, 1, 2
+SCHEDULE_TWO_PASS, SCHEDULE_L2_RING, SCHEDULE_ROW_BLOCKS, SCHEDULE_SHARED_ROW_BLOCKS = 0, 1, 2, 3
 _ERRNAMES = {-1: "MAG_E_ARG", -2: "MAG_E_RANGE", -3: "MAG_E_GEOMETRY", -4: "MAG_E_CUDA",
              -5: "MAG_E_TIMEOUT", -6: "MAG_E_NOMEM", -7: "MAG_E_UNSUPPORTED"}
 

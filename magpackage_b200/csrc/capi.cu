@@ -306,6 +306,7 @@ struct mag_mesh {
     int has_mat = 0;
     FusedPlan fused;
     RowBlockPlan rowblock;
+    RowBlockPlan rowshared;  // 128-incidence blocks with per-block distinct-element lists
     int schedule = MAG_SCHEDULE_ROW_BLOCKS;
     int64_t bytes = 0;
 
@@ -325,6 +326,7 @@ void destroy_mesh(mag_mesh *m) {
     free_pattern(&m->pat, nullptr);
     free_fused_plan(&m->fused);
     free_rowblock_plan(&m->rowblock);
+    free_rowblock_plan(&m->rowshared);
     cudaDeviceSynchronize();
     delete m;
 }
@@ -456,13 +458,22 @@ int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t N
         free_rowblock_plan(&m->rowblock);
         cudaGetLastError();
     }
+    if (build_rowblock_plan(m->rows(), &m->rowshared, s, kSharedBlockInc, true) == MAG_OK &&
+        m->rowshared.shared_ok) {
+        m->bytes += m->rowshared.bytes;
+    } else {
+        free_rowblock_plan(&m->rowshared);
+        cudaGetLastError();
+    }
     if (build_fused_plan(m->elems(), m->rows(), m->pat.max_row, &m->fused, s) == MAG_OK) {
         m->bytes += m->fused.bytes;
     } else {
         free_fused_plan(&m->fused);
         cudaGetLastError();
     }
-    m->schedule = m->rowblock.ok ? MAG_SCHEDULE_ROW_BLOCKS : MAG_SCHEDULE_TWO_PASS;
+    m->schedule = m->rowshared.shared_ok ? MAG_SCHEDULE_SHARED_ROW_BLOCKS
+                  : m->rowblock.ok        ? MAG_SCHEDULE_ROW_BLOCKS
+                                          : MAG_SCHEDULE_TWO_PASS;
     double qw[4], curl[72], val[72];
     default_reference_data(qw, curl, val);
     rc = make_quad(qw, 4, curl, val, &m->qp, &m->d_ref, s);
@@ -539,7 +550,12 @@ int mag_assemble_jacobian(mag_mesh *m, const double *d_sol, double *d_vals, doub
         return MAG_E_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    if (m->schedule == MAG_SCHEDULE_ROW_BLOCKS) {
+    if (m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS && m->rowshared.shared_ok && m->qp.standard_curl) {
+        MAG_TRY(launch_rowblock_shared_jacobian(m->rowshared, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp,
+                                                calc_j, calc_j ? d_vals : nullptr, d_res, s));
+        return finish(s);
+    }
+    if (m->schedule == MAG_SCHEDULE_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS) {
         MAG_TRY(launch_rowblock_jacobian(m->rowblock, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp, calc_j,
                                          calc_j ? d_vals : nullptr, d_res, s));
         return finish(s);
@@ -659,7 +675,8 @@ int mag_mesh_set_option(mag_mesh *m, int option, int64_t value) {
     }
     if (option == MAG_OPTION_SCHEDULE) {
         if ((value == MAG_SCHEDULE_L2_RING && !m->fused.ok) ||
-            (value == MAG_SCHEDULE_ROW_BLOCKS && !m->rowblock.ok) || value < 0 || value > 2) {
+            (value == MAG_SCHEDULE_ROW_BLOCKS && !m->rowblock.ok) ||
+            (value == MAG_SCHEDULE_SHARED_ROW_BLOCKS && !m->rowshared.shared_ok) || value < 0 || value > 3) {
             set_error("assembly schedule %lld is not available for this mesh", (long long)value);
             return MAG_E_UNSUPPORTED;
         }

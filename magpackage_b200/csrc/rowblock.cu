@@ -190,9 +190,247 @@ __global__ void __launch_bounds__(kBlockInc, 4) k_rowblock(RBArgs A) {
     }
 }
 
+// ---- shared-element variant --------------------------------------------------------
+
+// Per block: sort its (element, incidence) pairs, number the distinct elements in
+// ascending order, and record each incidence's slot. Counts above MAXE set *overflow.
+template <int BI, int MAXE>
+__global__ void __launch_bounds__(BI) k_block_elems(RowPlan rp, const int32_t *__restrict__ block_row,
+                                                           int32_t *__restrict__ blk_nelem,
+                                                           int32_t *__restrict__ blk_k0,
+                                                           int32_t *__restrict__ blk_elem,
+                                                           uint16_t *__restrict__ inc_slot, int *overflow) {
+    __shared__ unsigned long long key[BI];
+    __shared__ int scan[BI];
+    const int t = threadIdx.x;
+    const int a0 = block_row[blockIdx.x], a1 = block_row[blockIdx.x + 1];
+    const int k0 = rp.inc_ptr[a0], ninc = rp.inc_ptr[a1] - k0;
+    uint32_t ew = t < ninc ? rp.inc_elem[k0 + t] : 0xFFFFFFFFu;
+    key[t] = t < ninc ? ((unsigned long long)(ew & 0x1FFFFFFFu) << 8) | (unsigned)t : ~0ull;
+    __syncthreads();
+    // bitonic sort of BI keys
+    for (int k = 2; k <= BI; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int p = t ^ j;
+            if (p > t) {
+                unsigned long long x = key[t], y = key[p];
+                const bool up = (t & k) == 0;
+                if ((x > y) == up) {
+                    key[t] = y;
+                    key[p] = x;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const unsigned long long me = key[t];
+    const bool valid = me != ~0ull;
+    const bool first = valid && (t == 0 || (key[t - 1] >> 8) != (me >> 8));
+    scan[t] = first ? 1 : 0;
+    __syncthreads();
+    for (int off = 1; off < BI; off <<= 1) {  // inclusive scan
+        int v = t >= off ? scan[t - off] : 0;
+        __syncthreads();
+        scan[t] += v;
+        __syncthreads();
+    }
+    const int slot = scan[t] - 1;
+    if (valid) {
+        const int orig = (int)(me & 0xFF);
+        const uint32_t loc = rp.inc_elem[k0 + orig] >> 29;
+        inc_slot[k0 + orig] = (uint16_t)(slot | (loc << 8));
+        if (first) blk_elem[k0 + slot] = (int32_t)(me >> 8);
+    }
+    if (t == 0) {
+        blk_k0[blockIdx.x] = k0;
+        if (blockIdx.x == gridDim.x - 1) blk_k0[gridDim.x] = k0 + ninc;
+    }
+    if (t == BI - 1) {
+        blk_nelem[blockIdx.x] = scan[t];
+        if (overflow && scan[t] > MAXE) atomicExch(overflow, 1);
+    }
+}
+
+constexpr int kSv2 = 7;  // shared-memory stride (doubles) of one incidence's values
+
+// One distinct element of a block, evaluated once: what every row of the element needs.
+struct ElemRec {
+    double J[9];   // Jacobian columns (the standard curls are recomputed from these)
+    double r2;     // 2 / det
+    double b[6];   // B . C_j (unsigned curls)
+    double nu, g2; // nu(|B|^2), 2 d nu / d|B|^2
+    double adet;
+};
+
+// Shared-memory carve-up of one block of BI incidences with at most MAXE distinct elements.
+template <int BI, int MAXE>
+struct SharedLayout {
+    static constexpr int rec = (int)sizeof(ElemRec) * MAXE;  // phase B reuses it as the row accumulator
+    static constexpr int sv = 8 * BI * kSv2;
+    static constexpr int rsb = 4 * MAXE;
+    static constexpr int pos = 8 * BI;  // in-row positions (2 words per incidence when wide)
+    static constexpr int bytes = rec + sv + rsb + pos + 8 * (BI + 1);
+    static_assert(rec >= 8 * BI * 6, "the row accumulator reuses the element records");
+    static_assert(rec % 16 == 0 && sv % 16 == 0, "alignment of the shared-memory carve-up");
+};
+
+// Shared-element row blocks. Phase A1: one thread per distinct element of the block
+// gathers and evaluates it once (geometry, curls, B, nu(|B|^2)) into a shared record;
+// A2: one thread per incidence forms its element row from the record; B: one thread per
+// CSR row adds its incidences in ascending element order, as k_rowblock does, so the
+// bits are the same.
+template <int BI, int MAXE, int MINB, bool CALCJ, bool Q4, bool WIDE>
+__global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const int32_t *__restrict__ blk_nelem,
+                                                              const int32_t *__restrict__ blk_k0,
+                                                              const int32_t *__restrict__ blk_elem,
+                                                              const uint16_t *__restrict__ inc_slot) {
+    using L = SharedLayout<BI, MAXE>;
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    ElemRec *rec = reinterpret_cast<ElemRec *>(rs_smem);
+    double *sv = reinterpret_cast<double *>(rs_smem + L::rec);
+    unsigned *rsb = reinterpret_cast<unsigned *>(rs_smem + L::rec + L::sv);
+    uint32_t *spos = reinterpret_cast<uint32_t *>(rs_smem + L::rec + L::sv + L::rsb);
+    int *s_rp = reinterpret_cast<int *>(rs_smem + L::rec + L::sv + L::rsb + L::pos);
+    int *s_ip = s_rp + (BI + 1);
+    double *sacc = reinterpret_cast<double *>(rec);
+    const int tid = threadIdx.x;
+    // every prologue load depends only on the block index, so they all issue together
+    const int a0 = A.block_row[blockIdx.x], a1 = A.block_row[blockIdx.x + 1];
+    const int k0 = blk_k0[blockIdx.x], ninc = blk_k0[blockIdx.x + 1] - k0;
+    const int nel = blk_nelem[blockIdx.x];
+    const int nrows = a1 - a0;
+    const unsigned my_slot = tid < ninc ? inc_slot[k0 + tid] : 0u;
+    if (CALCJ && tid < ninc) {
+        if (WIDE) {
+            spos[2 * tid] = __ldg(A.rp.inc_pos + 2 * (int64_t)(k0 + tid));
+            spos[2 * tid + 1] = __ldg(A.rp.inc_pos + 2 * (int64_t)(k0 + tid) + 1);
+        } else {
+            spos[tid] = __ldg(A.rp.inc_pos + k0 + tid);
+        }
+    }
+    for (int r = tid; r <= nrows; r += BI) {
+        s_rp[r] = A.rp.row_ptr[a0 + r];
+        s_ip[r] = A.rp.inc_ptr[a0 + r];
+    }
+    // phase A1: one thread per distinct element (the plan keeps nel <= MAXE)
+    if (tid < nel && tid < MAXE) {
+        const int64_t e = blk_elem[k0 + tid];
+        int4 tt = A.m.tet[e];
+        int d[6];
+        load_dofs(A.m.dofs, e, d);
+        const unsigned sb = A.m.signbits ? A.m.signbits[e] : derived_signs(tt);
+        const int tag = A.m.tags[e];
+        Geo g;
+        geometry(A.m.xyz, tt, g);
+        double a[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) a[i] = d[i] >= 0 ? flip(__ldg(A.sol + d[i]), (sb >> i) & 1) : 0.0;
+        double C[6][3];
+        curls_standard(g, C);
+        double B[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double v = a[0] * C[0][c];
+#pragma unroll
+            for (int i = 1; i < 6; i++) v = v + a[i] * C[i][c];
+            B[c] = v;
+        }
+        double nu, dnu;
+        material_eval(A.mp, tag, dot3(B, B), nu, dnu);
+        ElemRec &R = rec[tid];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) R.J[3 * r + c] = g.J[r][c];
+        R.r2 = 2.0 * g.rdet;
+#pragma unroll
+        for (int j = 0; j < 6; j++) R.b[j] = dot3(B, C[j]);
+        R.nu = nu;
+        R.g2 = 2.0 * dnu;
+        R.adet = g.adet;
+        rsb[tid] = sb;
+    }
+    __syncthreads();
+    const int base = s_rp[0], span = s_rp[nrows] - base;
+    // phase A2: one thread per incidence, the element's row from its record
+    if (tid < ninc) {
+        const unsigned sl = my_slot;
+        const ElemRec &R = rec[sl & 0xFF];
+        const int loc = (int)(sl >> 8);
+        const unsigned sb = rsb[sl & 0xFF];
+        Geo g;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) g.J[r][c] = R.J[3 * r + c];
+        g.rdet = 0.5 * R.r2;  // exact: curls_standard forms 2 * rdet again
+        g.adet = R.adet;
+        double C[6][3];
+        curls_standard(g, C);
+        const unsigned si = (sb >> loc) & 1;
+        const double w0 = A.qp.qw[0] * R.adet, nu = R.nu;
+        double Cl[3];
+        pick(C, loc, Cl);
+        double bl = R.b[0];
+#pragma unroll
+        for (int j = 1; j < 6; j++) bl = loc == j ? R.b[j] : bl;
+        double *out = sv + tid * kSv2;
+        out[6] = flip(qsum_w<Q4>(nu * bl, A.qp, w0, R.adet), si);
+        if (CALCJ) {
+            if (R.g2 == 0.0) {
+#pragma unroll
+                for (int j = 0; j < 6; j++)
+                    out[j] = flip(qsum_w<Q4>(nu * dot3(Cl, C[j]), A.qp, w0, R.adet), si ^ ((sb >> j) & 1));
+            } else {
+                const double gl = R.g2 * bl;
+#pragma unroll
+                for (int j = 0; j < 6; j++)
+                    out[j] = flip(qsum_w<Q4>(nu * dot3(Cl, C[j]) + gl * R.b[j], A.qp, w0, R.adet),
+                                  si ^ ((sb >> j) & 1));
+            }
+        }
+    }
+    __syncthreads();  // the records are dead from here on; sacc reuses their memory
+    if (CALCJ) {
+        for (int i = tid; i < span; i += BI) sacc[i] = 0.0;
+        __syncthreads();
+    }
+    // phase B: one thread per row adds its incidences in ascending element order
+    for (int r = tid; r < nrows; r += BI) {
+        const int off = s_rp[r] - base;
+        double racc = 0.0;
+        for (int k = s_ip[r]; k < s_ip[r + 1]; k++) {
+            const double *v = sv + (k - k0) * kSv2;
+            if (CALCJ) {
+                if (!WIDE) {
+                    uint32_t pw = spos[k - k0];
+#pragma unroll
+                    for (int j = 0; j < 6; j++) {
+                        uint32_t p = (pw >> (5 * j)) & 31u;
+                        if (p != (uint32_t)kCompactMaxRow) sacc[off + p] = sacc[off + p] + v[j];
+                    }
+                } else {
+                    uint32_t w0 = spos[2 * (k - k0)], w1 = spos[2 * (k - k0) + 1];
+#pragma unroll
+                    for (int j = 0; j < 6; j++) {
+                        uint32_t p = (j < 4 ? (w0 >> (8 * j)) : (w1 >> (8 * (j - 4)))) & 255u;
+                        if (p != (uint32_t)kWideMaxRow) sacc[off + p] = sacc[off + p] + v[j];
+                    }
+                }
+            }
+            racc = racc + v[6];
+        }
+        A.res[a0 + r] = racc;
+    }
+    if (CALCJ) {
+        __syncthreads();
+        for (int i = tid; i < span; i += BI) A.vals[base + i] = sacc[i];
+    }
+}
+
 }  // namespace
 
-int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc) {
+int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc, bool with_shared) {
     *out = RowBlockPlan{};
     std::vector<int32_t> ip((size_t)rp.ndof + 1);
     MAG_CUDA_TRY(cudaMemcpyAsync(ip.data(), rp.inc_ptr, ip.size() * 4, cudaMemcpyDeviceToHost, s));
@@ -212,17 +450,94 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
         a = b;
     }
     starts.push_back((int32_t)rp.ndof);
-    out->nblocks = (int32_t)starts.size() - 1;
-    MAG_CUDA_TRY(cudaMalloc(&out->block_row, starts.size() * 4));
-    MAG_CUDA_TRY(cudaMemcpyAsync(out->block_row, starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, s));
+    out->block_inc = block_inc;
+    const int64_t ninc = ip[rp.ndof];
+    const int max_elems = block_inc == kSharedBlockInc ? kSharedMaxElems : kMaxBlockElems;
+    with_shared = with_shared && (block_inc == kSharedBlockInc || block_inc == kBlockInc);
+    if (with_shared) {
+        if (cudaMalloc(&out->blk_elem, (size_t)(ninc > 0 ? ninc : 1) * 4) != cudaSuccess ||
+            cudaMalloc(&out->inc_slot, (size_t)(ninc > 0 ? ninc : 1) * 2) != cudaSuccess)
+            with_shared = false;
+    }
+    // Upload the blocks; for the shared-element lists, split any block whose distinct
+    // elements exceed the kernel's capacity and rebuild (a few passes at most).
+    for (int pass = 0;; pass++) {
+        out->nblocks = (int32_t)starts.size() - 1;
+        if (out->block_row) cudaFree(out->block_row);
+        if (out->blk_nelem) cudaFree(out->blk_nelem);
+        if (out->blk_k0) cudaFree(out->blk_k0);
+        out->block_row = nullptr;
+        out->blk_nelem = nullptr;
+        out->blk_k0 = nullptr;
+        MAG_CUDA_TRY(cudaMalloc(&out->block_row, starts.size() * 4));
+        MAG_CUDA_TRY(cudaMemcpyAsync(out->block_row, starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, s));
+        if (!with_shared) break;
+        if (cudaMalloc(&out->blk_nelem, (size_t)out->nblocks * 4) != cudaSuccess ||
+            cudaMalloc(&out->blk_k0, (size_t)(out->nblocks + 1) * 4) != cudaSuccess) {
+            with_shared = false;
+            break;
+        }
+        if (block_inc == kSharedBlockInc)
+            k_block_elems<kSharedBlockInc, kSharedMaxElems><<<out->nblocks, kSharedBlockInc, 0, s>>>(
+                rp, out->block_row, out->blk_nelem, out->blk_k0, out->blk_elem, out->inc_slot, nullptr);
+        else
+            k_block_elems<kBlockInc, kMaxBlockElems><<<out->nblocks, kBlockInc, 0, s>>>(
+                rp, out->block_row, out->blk_nelem, out->blk_k0, out->blk_elem, out->inc_slot, nullptr);
+        std::vector<int32_t> nel((size_t)out->nblocks);
+        if (cudaMemcpyAsync(nel.data(), out->blk_nelem, nel.size() * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            with_shared = false;
+            break;
+        }
+        std::vector<int32_t> next;
+        next.reserve(starts.size() + 16);
+        bool split = false;
+        for (int32_t b = 0; b < out->nblocks; b++) {
+            next.push_back(starts[b]);
+            if (nel[b] > max_elems && starts[b + 1] - starts[b] > 1) {
+                next.push_back(starts[b] + (starts[b + 1] - starts[b]) / 2);
+                split = true;
+            } else if (nel[b] > max_elems) {
+                with_shared = false;  // one row alone exceeds the capacity
+            }
+        }
+        next.push_back(starts.back());
+        if (!with_shared) break;
+        if (!split) {
+            out->shared_ok = 1;
+            break;
+        }
+        if (pass >= 4) {
+            with_shared = false;
+            break;
+        }
+        starts.swap(next);
+    }
     MAG_CUDA_TRY(cudaStreamSynchronize(s));
-    out->bytes = (int64_t)starts.size() * 4;
     out->ok = 1;
+    out->bytes = (int64_t)starts.size() * 4;
+    if (out->shared_ok) {
+        out->bytes += (int64_t)out->nblocks * 8 + ninc * 6;
+    } else {
+        cudaGetLastError();
+        if (out->blk_nelem) cudaFree(out->blk_nelem);
+        if (out->blk_k0) cudaFree(out->blk_k0);
+        if (out->blk_elem) cudaFree(out->blk_elem);
+        if (out->inc_slot) cudaFree(out->inc_slot);
+        out->blk_nelem = nullptr;
+        out->blk_k0 = nullptr;
+        out->blk_elem = nullptr;
+        out->inc_slot = nullptr;
+    }
     return MAG_OK;
 }
 
 void free_rowblock_plan(RowBlockPlan *p) {
     if (p->block_row) cudaFree(p->block_row);
+    if (p->blk_nelem) cudaFree(p->blk_nelem);
+    if (p->blk_k0) cudaFree(p->blk_k0);
+    if (p->blk_elem) cudaFree(p->blk_elem);
+    if (p->inc_slot) cudaFree(p->inc_slot);
     *p = RowBlockPlan{};
 }
 
@@ -252,6 +567,47 @@ int launch_rowblock_jacobian(const RowBlockPlan &bp, const ElemData &m, const Ro
     cudaError_t e = cudaPeekAtLastError();
     if (e != cudaSuccess) {
         set_error("row-block launch: %s", cudaGetErrorString(e));
+        return MAG_E_CUDA;
+    }
+    return MAG_OK;
+}
+
+}  // namespace mag
+
+namespace mag {
+
+int launch_rowblock_shared_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp,
+                                    const double *sol, const QuadParams &qp, const MaterialParams &mp, int calcj,
+                                    double *vals, double *res, cudaStream_t s) {
+    if (!bp.ok || !bp.shared_ok || !qp.standard_curl) return MAG_E_UNSUPPORTED;
+    RBArgs A{m, rp, sol, qp, mp, bp.block_row, vals, res};
+    const bool wide = rp.wide != 0, q4 = qp.nq == 4 && qp.uniform_w;
+#define MAG_RS(BI_, ME_, MB_, CJ, Q, W)                                                                   \
+    do {                                                                                                 \
+        auto kern = k_rowblock_shared<BI_, ME_, MB_, CJ, Q, W>;                                          \
+        const int sm = SharedLayout<BI_, ME_>::bytes;                                                    \
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                     \
+        kern<<<bp.nblocks, BI_, sm, s>>>(A, bp.blk_nelem, bp.blk_k0, bp.blk_elem, bp.inc_slot);          \
+    } while (0)
+#define MAG_RS_ALL(BI_, ME_, MB_)                                                                         \
+    do {                                                                                                 \
+        if (calcj) {                                                                                     \
+            if (q4) {                                                                                    \
+                if (wide) MAG_RS(BI_, ME_, MB_, true, true, true); else MAG_RS(BI_, ME_, MB_, true, true, false); \
+            } else {                                                                                     \
+                if (wide) MAG_RS(BI_, ME_, MB_, true, false, true); else MAG_RS(BI_, ME_, MB_, true, false, false); \
+            }                                                                                            \
+        } else {                                                                                         \
+            if (q4) MAG_RS(BI_, ME_, MB_, false, true, false); else MAG_RS(BI_, ME_, MB_, false, false, false); \
+        }                                                                                                \
+    } while (0)
+    if (bp.block_inc == kSharedBlockInc) MAG_RS_ALL(kSharedBlockInc, kSharedMaxElems, 4);
+    else MAG_RS_ALL(kBlockInc, kMaxBlockElems, 4);
+#undef MAG_RS_ALL
+#undef MAG_RS
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        set_error("shared row-block launch: %s", cudaGetErrorString(e));
         return MAG_E_CUDA;
     }
     return MAG_OK;

@@ -11,17 +11,35 @@ namespace mag {
 
 constexpr int kBlockInc = 256;  // incidences per CTA == threads per CTA
 
+constexpr int kMaxBlockElems = 224;  // distinct elements per 256-incidence block the shared kernel holds
+constexpr int kSharedBlockInc = 256; // block size of the shared-element schedule (4 CTAs per SM)
+constexpr int kSharedMaxElems = 224; // distinct elements per block (larger blocks are split)
+
 struct RowBlockPlan {
     int32_t *block_row = nullptr;  // [nblocks+1]
     int32_t nblocks = 0;
     int64_t bytes = 0;
     int ok = 0;
+    int block_inc = 0;
+    // shared-element variant: each block's distinct elements, ascending, stored at the
+    // block's first incidence offset; per incidence its slot in that list and local row
+    int32_t *blk_nelem = nullptr;  // [nblocks]
+    int32_t *blk_k0 = nullptr;     // [nblocks+1] first incidence of each block
+    int32_t *blk_elem = nullptr;   // [ninc] (first blk_nelem[b] entries after the block's offset)
+    uint16_t *inc_slot = nullptr;  // [ninc] slot | local row << 8
+    int shared_ok = 0;
 };
 
-int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc = kBlockInc);
+int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc = kBlockInc,
+                        bool with_shared = false);
 void free_rowblock_plan(RowBlockPlan *p);
 int launch_rowblock_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *sol,
                              const QuadParams &qp, const MaterialParams &mp, int calcj, double *vals,
                              double *res, cudaStream_t s);
+// Same result, bit for bit, with each block's distinct elements evaluated once
+// (standard curl table only; needs bp.shared_ok).
+int launch_rowblock_shared_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp,
+                                    const double *sol, const QuadParams &qp, const MaterialParams &mp, int calcj,
+                                    double *vals, double *res, cudaStream_t s);
 
 }  // namespace mag

@@ -351,17 +351,19 @@ def test_errors_are_reported(oracle_port):
 
 # ---- the three Jacobian schedules ------------------------------------------------------------
 
-SCHEDULES = (_lib.SCHEDULE_ROW_BLOCKS, _lib.SCHEDULE_L2_RING, _lib.SCHEDULE_TWO_PASS)
+SCHEDULES = (_lib.SCHEDULE_SHARED_ROW_BLOCKS, _lib.SCHEDULE_ROW_BLOCKS, _lib.SCHEDULE_L2_RING,
+             _lib.SCHEDULE_TWO_PASS)
 
 
 @pytest.mark.parametrize("n,seed", [(13, 21), (30, 22)])
 def test_schedules_agree_bit_for_bit(oracle_port, n, seed):
-    """Row blocks (default), the persistent L2-ring launch (ring reused many times at 30^3)
-    and the two-pass kernels give the same bits as each other and as the oracle, with and
-    without the Jacobian, on the fast and the general quadrature path."""
+    """Shared-element row blocks (default), per-incidence row blocks, the persistent L2-ring
+    launch (ring reused many times at 30^3) and the two-pass kernels give the same bits as
+    each other and as the oracle, with and without the Jacobian, on the fast and the general
+    quadrature path."""
     mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, n, seed)
     plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
-    assert plan.info.schedule == _lib.SCHEDULE_ROW_BLOCKS
+    assert plan.info.schedule == _lib.SCHEDULE_SHARED_ROW_BLOCKS
     if n >= 30:
         assert 2 * plan.info.fused_ring_tiles < (mesh.num_elements + 255) // 256
     pk = material.pack_material_data(synth.standard_materials())
