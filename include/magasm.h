@@ -200,9 +200,11 @@ int mag_batch_destroy(mag_batch *batch);
  * tensor cores (BF16 operands, FP32 accumulation in tensor memory) with FP32
  * master weights and Adam. It predicts log-reluctivity per element from the
  * previous steps' |B|, the source and the material, to seed the first Jacobian
- * of a Newton solve through the per-element nu entry (mag_assemble_stiffness,
- * the Assembler.assembleStiffness(space, nu_vec) path, src/Assembler.m:26-39).
- * Parameters: W1[64][4] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4. */
+ * of a Newton solve (mag_seed_midpoint + mag_assemble_jacobian_seeded).
+ * Parameters: W1[64][4] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4.
+ * Feature arrays are [rows][4] float32 and 16-byte aligned. SiLU is evaluated
+ * with the hardware tanh approximation (relative error ~2^-11, below the BF16
+ * rounding of every layer input). */
 typedef struct mag_mlp mag_mlp;
 int mag_mlp_num_params(void);
 int mag_mlp_create(const float *init_params, mag_mlp **out);

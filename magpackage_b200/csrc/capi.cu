@@ -935,7 +935,7 @@ int mag_mlp_set_params(mag_mlp *n, const float *host) {
 }
 
 int mag_mlp_forward(mag_mlp *n, const float *d_feats, int64_t rows, float *d_y, float *d_z, void *stream) {
-    if (!n || !d_feats || rows <= 0 || !d_y) {
+    if (!n || !d_feats || rows <= 0 || !d_y || ((uintptr_t)d_feats & 15)) {
         set_error("mag_mlp_forward: bad arguments");
         return MAG_E_ARG;
     }
@@ -945,7 +945,7 @@ int mag_mlp_forward(mag_mlp *n, const float *d_feats, int64_t rows, float *d_y, 
 
 int mag_mlp_predict_nu(mag_mlp *n, const float *d_feats, int64_t rows, const int32_t *d_rows, double y_scale,
                        double y_shift, double nu_min, double nu_max, double *d_nu, void *stream) {
-    if (!n || !d_feats || rows <= 0 || !d_nu || !(nu_min > 0) || !(nu_max >= nu_min)) {
+    if (!n || !d_feats || rows <= 0 || !d_nu || !(nu_min > 0) || !(nu_max >= nu_min) || ((uintptr_t)d_feats & 15)) {
         set_error("mag_mlp_predict_nu: bad arguments");
         return MAG_E_ARG;
     }
@@ -956,7 +956,7 @@ int mag_mlp_predict_nu(mag_mlp *n, const float *d_feats, int64_t rows, const int
 
 int mag_mlp_gradient(mag_mlp *n, const float *d_feats, const float *d_target, int64_t rows, float loss_scale,
                      float *d_y, float *d_z, float *d_grad, void *stream) {
-    if (!n || !d_feats || !d_target || rows <= 0 || !d_y || !d_z) {
+    if (!n || !d_feats || !d_target || rows <= 0 || !d_y || !d_z || ((uintptr_t)d_feats & 15)) {
         set_error("mag_mlp_gradient: bad arguments");
         return MAG_E_ARG;
     }

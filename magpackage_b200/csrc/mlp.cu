@@ -46,9 +46,16 @@ __host__ __device__ constexpr int core_off(int r, int k, int K) {
     return (r >> 3) * (K * 8) + (k >> 3) * 64 + (r & 7) * 8 + (k & 7);
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// sigmoid(z) = (1 + tanh(z/2)) / 2 with the hardware tanh approximation (one MUFU
+// operation; relative error about 2^-11, below the BF16 rounding every layer input gets).
+__device__ __forceinline__ float sigmoid_fast(float z) {
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
+    return 0.5f + 0.5f * t;
+}
+__device__ __forceinline__ float silu(float z) { return z * sigmoid_fast(z); }
 __device__ __forceinline__ float dsilu(float z) {
-    float s = 1.0f / (1.0f + __expf(-z));
+    float s = sigmoid_fast(z);
     return s * (1.0f + z * (1.0f - s));
 }
 
@@ -108,30 +115,32 @@ __device__ __forceinline__ void mma_issue(uint32_t tmem, const __nv_bfloat16 *A,
                  : "memory");
 }
 
-// This thread's accumulator row (64 FP32 columns) from TMEM.
+// This thread's accumulator row (64 FP32 columns) from TMEM: four 16-column loads
+// in flight, one wait.
 __device__ __forceinline__ void tmem_row(uint32_t tmem, float out[kH]) {
     const uint32_t lane_base = (uint32_t)((threadIdx.x >> 5) * 32) << 16;
+    uint32_t r[kH];
 #pragma unroll
     for (int c = 0; c < kH; c += 16) {
-        uint32_t r[16];
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "=r"(r[c + 0]), "=r"(r[c + 1]), "=r"(r[c + 2]), "=r"(r[c + 3]), "=r"(r[c + 4]), "=r"(r[c + 5]),
+              "=r"(r[c + 6]), "=r"(r[c + 7]), "=r"(r[c + 8]), "=r"(r[c + 9]), "=r"(r[c + 10]), "=r"(r[c + 11]),
+              "=r"(r[c + 12]), "=r"(r[c + 13]), "=r"(r[c + 14]), "=r"(r[c + 15])
             : "r"(tmem + lane_base + (uint32_t)c));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int i = 0; i < 16; i++) out[c + i] = __uint_as_float(r[i]);
     }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < kH; i++) out[i] = __uint_as_float(r[i]);
 }
 
 // Write this thread's row of 64 values as BF16 into a K=64 core-matrix image.
 __device__ __forceinline__ void put_row64(__nv_bfloat16 *img, int row, const float v[kH]) {
 #pragma unroll
     for (int kb = 0; kb < 8; kb++) {
-        __align__(16) __nv_bfloat16 t[8];
+        __align__(16) __nv_bfloat162 t[4];
 #pragma unroll
-        for (int i = 0; i < 8; i++) t[i] = __float2bfloat16_rn(v[kb * 8 + i]);
+        for (int i = 0; i < 4; i++) t[i] = __floats2bfloat162_rn(v[kb * 8 + 2 * i], v[kb * 8 + 2 * i + 1]);
         *reinterpret_cast<uint4 *>(img + core_off(row, kb * 8, kH)) = *reinterpret_cast<uint4 *>(t);
     }
 }
@@ -139,6 +148,7 @@ __device__ __forceinline__ void put_row64(__nv_bfloat16 *img, int row, const flo
 struct Smem {
     __nv_bfloat16 act[kRows * kH];      // layer input image (K=64) or the K=16 input image
     __nv_bfloat16 w[2 * kWElems + kW1pElems];
+    float vec[4 * kH + 1];              // b1 | b2 | b3 | w4 | b4 (forward kernel)
     uint64_t bar;
     uint32_t tmem;
     int fail;
@@ -198,18 +208,30 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp_forward(MlpForwardArgs a) {
     }
     // all weight images: W1p | W2 | W3 (contiguous in the operand buffer)
     load_ops(S, a.ops, bW1p, kW1pElems + 2 * kWElems);
+    for (int i = t; i < kH; i += kRows) {
+        S.vec[i] = a.params[ob1 + i];
+        S.vec[kH + i] = a.params[ob2 + i];
+        S.vec[2 * kH + i] = a.params[ob3 + i];
+        S.vec[3 * kH + i] = a.params[ow4 + i];
+    }
+    if (t == 0) S.vec[4 * kH] = a.params[ob4];
     tmem_alloc(S);
     __syncthreads();
     tc_fence_after();
     const __nv_bfloat16 *W1 = S.w, *W2 = S.w + kW1pElems, *W3 = S.w + kW1pElems + kWElems;
-    const float *P = a.params;
+    const float *sb1 = S.vec, *sb2 = S.vec + kH, *sb3 = S.vec + 2 * kH, *sw4 = S.vec + 3 * kH;
     uint32_t phase = 0;
     for (int tile = blockIdx.x; tile * kRows < a.n; tile += gridDim.x) {
         const int64_t row = (int64_t)tile * kRows + t;
         const bool valid = row < a.n;
         float x[4] = {0, 0, 0, 0};
-        if (valid)
-            for (int i = 0; i < 4; i++) x[i] = a.feats[row * 4 + i];
+        if (valid) {  // one 16-byte load per row (feature rows are 16 bytes, the buffer 16-byte aligned)
+            const float4 f = __ldg(reinterpret_cast<const float4 *>(a.feats) + row);
+            x[0] = f.x;
+            x[1] = f.y;
+            x[2] = f.z;
+            x[3] = f.w;
+        }
         {  // input image, K = 16 (features 4..15 are zero)
             __align__(16) __nv_bfloat16 v[16];
             for (int i = 0; i < 16; i++) v[i] = __float2bfloat16_rn(i < 4 ? x[i] : 0.0f);
@@ -222,7 +244,7 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp_forward(MlpForwardArgs a) {
         tmem_row(S.tmem, z);
 #pragma unroll
         for (int o = 0; o < kH; o++) {
-            z[o] += P[ob1 + o];
+            z[o] += sb1[o];
             h[o] = silu(z[o]);
         }
         if (a.z_out && valid)
@@ -235,7 +257,7 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp_forward(MlpForwardArgs a) {
         tmem_row(S.tmem, z);
 #pragma unroll
         for (int o = 0; o < kH; o++) {
-            z[o] += P[ob2 + o];
+            z[o] += sb2[o];
             h[o] = silu(z[o]);
         }
         if (a.z_out && valid)
@@ -249,10 +271,10 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp_forward(MlpForwardArgs a) {
         float y = 0.0f;
 #pragma unroll
         for (int o = 0; o < kH; o++) {
-            z[o] += P[ob3 + o];
-            y += P[ow4 + o] * silu(z[o]);
+            z[o] += sb3[o];
+            y += sw4[o] * silu(z[o]);
         }
-        y += P[ob4];
+        y += S.vec[4 * kH];
         if (a.z_out && valid)
             for (int o = 0; o < kH; o++) a.z_out[(row * 3 + 2) * kH + o] = z[o];
         if (valid) {
