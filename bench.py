@@ -266,7 +266,7 @@ def main():
                     choices=sorted(WORKLOADS) + ["batched_complex", "transient"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--schedule", default="shared-row-blocks",
-                    choices=["shared-row-blocks", "row-blocks", "l2-ring", "two-pass"],
+                    choices=["shared-row-blocks", "staged-row-blocks", "row-blocks", "l2-ring", "two-pass"],
                     help="Jacobian assembly schedule (all give identical bits)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -306,6 +306,7 @@ def main():
     plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
     plan.set_materials(packed)
     sched_id = {"shared-row-blocks": _lib.SCHEDULE_SHARED_ROW_BLOCKS,
+                "staged-row-blocks": _lib.SCHEDULE_STAGED_ROW_BLOCKS,
                 "row-blocks": _lib.SCHEDULE_ROW_BLOCKS, "l2-ring": _lib.SCHEDULE_L2_RING,
                 "two-pass": _lib.SCHEDULE_TWO_PASS}[args.schedule]
     plan.set_schedule(sched_id)
@@ -428,7 +429,11 @@ def main():
             "config": {"workload": desc, "elements": ne, "edges": E, "nnz": nnz,
                        "l2": "inputs larger than L2 (per-step working set > 700 MB)",
                        "parallelism": f"{world} independent instance(s)",
-                       "schedule": {_lib.SCHEDULE_SHARED_ROW_BLOCKS: "row blocks: one launch, no scratch, "
+                       "shared_blocks": plan.info.shared_blocks, "shared_staged": plan.info.shared_staged,
+                       "schedule": {_lib.SCHEDULE_STAGED_ROW_BLOCKS: "row blocks with shared elements, the "
+                                                                     "block's nodes and edge values staged in "
+                                                                     "shared memory first",
+                                    _lib.SCHEDULE_SHARED_ROW_BLOCKS: "row blocks: one launch, no scratch, "
                                                                      "each block's distinct elements "
                                                                      "evaluated once in shared memory",
                                     _lib.SCHEDULE_ROW_BLOCKS: "row blocks: one launch, per-row element "

@@ -458,7 +458,8 @@ int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t N
         free_rowblock_plan(&m->rowblock);
         cudaGetLastError();
     }
-    if (build_rowblock_plan(m->rows(), &m->rowshared, s, kSharedBlockInc, true) == MAG_OK &&
+    const ElemData ed = m->elems();
+    if (build_rowblock_plan(m->rows(), &m->rowshared, s, kSharedBlockInc, true, &ed) == MAG_OK &&
         m->rowshared.shared_ok) {
         m->bytes += m->rowshared.bytes;
     } else {
@@ -505,6 +506,8 @@ int mag_mesh_get_info(const mag_mesh *m, mag_mesh_info *info) {
     info->fused_ring_tiles = m->fused.ring_tiles;
     info->fused_grid = m->fused.grid;
     info->device_bytes = m->bytes;
+    info->shared_blocks = m->rowshared.shared_ok ? m->rowshared.nblocks : 0;
+    info->shared_staged = m->rowshared.staged_ok;
     return MAG_OK;
 }
 
@@ -550,12 +553,13 @@ int mag_assemble_jacobian(mag_mesh *m, const double *d_sol, double *d_vals, doub
         return MAG_E_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    if (m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS && m->rowshared.shared_ok && m->qp.standard_curl) {
+    const bool staged = m->schedule == MAG_SCHEDULE_STAGED_ROW_BLOCKS;
+    if ((m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || staged) && m->rowshared.shared_ok && m->qp.standard_curl) {
         MAG_TRY(launch_rowblock_shared_jacobian(m->rowshared, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp,
-                                                calc_j, calc_j ? d_vals : nullptr, d_res, s));
+                                                calc_j, calc_j ? d_vals : nullptr, d_res, s, staged));
         return finish(s);
     }
-    if (m->schedule == MAG_SCHEDULE_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS) {
+    if (m->schedule == MAG_SCHEDULE_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || staged) {
         MAG_TRY(launch_rowblock_jacobian(m->rowblock, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp, calc_j,
                                          calc_j ? d_vals : nullptr, d_res, s));
         return finish(s);
@@ -676,7 +680,8 @@ int mag_mesh_set_option(mag_mesh *m, int option, int64_t value) {
     if (option == MAG_OPTION_SCHEDULE) {
         if ((value == MAG_SCHEDULE_L2_RING && !m->fused.ok) ||
             (value == MAG_SCHEDULE_ROW_BLOCKS && !m->rowblock.ok) ||
-            (value == MAG_SCHEDULE_SHARED_ROW_BLOCKS && !m->rowshared.shared_ok) || value < 0 || value > 3) {
+            (value == MAG_SCHEDULE_SHARED_ROW_BLOCKS && !m->rowshared.shared_ok) ||
+            (value == MAG_SCHEDULE_STAGED_ROW_BLOCKS && !m->rowshared.staged_ok) || value < 0 || value > 4) {
             set_error("assembly schedule %lld is not available for this mesh", (long long)value);
             return MAG_E_UNSUPPORTED;
         }

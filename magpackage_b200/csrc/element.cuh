@@ -27,8 +27,7 @@ struct Geo {
     double det, rdet, adet;
 };
 
-__device__ __forceinline__ void geometry(const double4 *__restrict__ xyz, int4 t, Geo &g) {
-    double4 v0 = xyz[t.x], v1 = xyz[t.y], v2 = xyz[t.z], v3 = xyz[t.w];
+__device__ __forceinline__ void geometry_v(double4 v0, double4 v1, double4 v2, double4 v3, Geo &g) {
     g.J[0][0] = v1.x - v0.x; g.J[1][0] = v1.y - v0.y; g.J[2][0] = v1.z - v0.z;
     g.J[0][1] = v2.x - v0.x; g.J[1][1] = v2.y - v0.y; g.J[2][1] = v2.z - v0.z;
     g.J[0][2] = v3.x - v0.x; g.J[1][2] = v3.y - v0.y; g.J[2][2] = v3.z - v0.z;
@@ -39,6 +38,10 @@ __device__ __forceinline__ void geometry(const double4 *__restrict__ xyz, int4 t
     g.det = J[0][0] * m0 - J[0][1] * m1 + J[0][2] * m2;
     g.rdet = 1.0 / g.det;
     g.adet = fabs(g.det);
+}
+
+__device__ __forceinline__ void geometry(const double4 *__restrict__ xyz, int4 t, Geo &g) {
+    geometry_v(xyz[t.x], xyz[t.y], xyz[t.z], xyz[t.w], g);
 }
 
 // Physical curls of the six Whitney functions, C_i = J c_i / det, for the

@@ -470,6 +470,8 @@ int build_fused_plan(const ElemData &m, const RowPlan &rp, int max_row, FusedPla
     MAG_CUDA_TRY(cudaMalloc(&fp->sched, sched.size() * 4));
     MAG_CUDA_TRY(cudaMalloc(&fp->need, need.size() * 4));
     MAG_CUDA_TRY(cudaMalloc(&fp->ctrl, fp->ctrl_bytes));
+    // the status word is read by mag_mesh_check whichever schedule ran: start it clear
+    MAG_CUDA_TRY(cudaMemsetAsync(fp->ctrl, 0, fp->ctrl_bytes, s));
     MAG_CUDA_TRY(cudaMalloc(&fp->ring, ring_bytes));
     MAG_CUDA_TRY(cudaMemcpyAsync(fp->sched, sched.data(), sched.size() * 4, cudaMemcpyHostToDevice, s));
     MAG_CUDA_TRY(cudaMemcpyAsync(fp->need, need.data(), need.size() * 4, cudaMemcpyHostToDevice, s));

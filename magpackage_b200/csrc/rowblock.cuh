@@ -28,10 +28,21 @@ struct RowBlockPlan {
     int32_t *blk_elem = nullptr;   // [ninc] (first blk_nelem[b] entries after the block's offset)
     uint16_t *inc_slot = nullptr;  // [ninc] slot | local row << 8
     int shared_ok = 0;
+    // staging: per block its distinct nodes and edge dofs, and per distinct element a
+    // record of local node / edge indices, tag and sign bits (exact offsets per block)
+    int32_t *stg_cnt = nullptr;    // [nblocks][2] nodes, edges
+    int32_t *stg_off = nullptr;    // [nblocks][3] node, edge, element-record offsets
+    int32_t *stg_node = nullptr;   // node ids
+    int32_t *stg_edge = nullptr;   // edge dofs
+    uint4 *stg_erec = nullptr;     // element records
+    int staged_ok = 0;
 };
 
+constexpr int kStageMaxNodes = 192;  // distinct nodes per block the staged kernel holds
+constexpr int kStageMaxEdges = 512;  // distinct edge dofs per block
+
 int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc = kBlockInc,
-                        bool with_shared = false);
+                        bool with_shared = false, const ElemData *stage_mesh = nullptr);
 void free_rowblock_plan(RowBlockPlan *p);
 int launch_rowblock_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *sol,
                              const QuadParams &qp, const MaterialParams &mp, int calcj, double *vals,
@@ -40,6 +51,6 @@ int launch_rowblock_jacobian(const RowBlockPlan &bp, const ElemData &m, const Ro
 // (standard curl table only; needs bp.shared_ok).
 int launch_rowblock_shared_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp,
                                     const double *sol, const QuadParams &qp, const MaterialParams &mp, int calcj,
-                                    double *vals, double *res, cudaStream_t s);
+                                    double *vals, double *res, cudaStream_t s, bool staged = false);
 
 }  // namespace mag

@@ -351,8 +351,8 @@ def test_errors_are_reported(oracle_port):
 
 # ---- the three Jacobian schedules ------------------------------------------------------------
 
-SCHEDULES = (_lib.SCHEDULE_SHARED_ROW_BLOCKS, _lib.SCHEDULE_ROW_BLOCKS, _lib.SCHEDULE_L2_RING,
-             _lib.SCHEDULE_TWO_PASS)
+SCHEDULES = (_lib.SCHEDULE_SHARED_ROW_BLOCKS, _lib.SCHEDULE_STAGED_ROW_BLOCKS, _lib.SCHEDULE_ROW_BLOCKS,
+             _lib.SCHEDULE_L2_RING, _lib.SCHEDULE_TWO_PASS)
 
 
 @pytest.mark.parametrize("n,seed", [(13, 21), (30, 22)])
@@ -363,7 +363,7 @@ def test_schedules_agree_bit_for_bit(oracle_port, n, seed):
     quadrature path."""
     mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, n, seed)
     plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
-    assert plan.info.schedule == _lib.SCHEDULE_SHARED_ROW_BLOCKS
+    assert plan.info.schedule == _lib.SCHEDULE_SHARED_ROW_BLOCKS and plan.info.shared_staged == 1
     if n >= 30:
         assert 2 * plan.info.fused_ring_tiles < (mesh.num_elements + 255) // 256
     pk = material.pack_material_data(synth.standard_materials())
