@@ -199,7 +199,8 @@ __global__ void __launch_bounds__(BI) k_block_elems(RowPlan rp, const int32_t *_
                                                            int32_t *__restrict__ blk_nelem,
                                                            int32_t *__restrict__ blk_k0,
                                                            int32_t *__restrict__ blk_elem,
-                                                           uint16_t *__restrict__ inc_slot, int *overflow) {
+                                                           uint16_t *__restrict__ inc_slot,
+                                                           uint32_t *__restrict__ inc_sorted, int *overflow) {
     __shared__ unsigned long long key[BI];
     __shared__ int scan[BI];
     const int t = threadIdx.x;
@@ -239,6 +240,7 @@ __global__ void __launch_bounds__(BI) k_block_elems(RowPlan rp, const int32_t *_
         const int orig = (int)(me & 0xFF);
         const uint32_t loc = rp.inc_elem[k0 + orig] >> 29;
         inc_slot[k0 + orig] = (uint16_t)(slot | (loc << 8));
+        if (inc_sorted) inc_sorted[k0 + t] = (uint32_t)slot | loc << 8 | (uint32_t)orig << 16;
         if (first) blk_elem[k0 + slot] = (int32_t)(me >> 8);
     }
     if (t == 0) {
@@ -403,7 +405,7 @@ struct SharedLayout {
     static constexpr int rsb = 4 * MAXE;
     static constexpr int pos = 8 * BI;  // in-row positions (2 words per incidence when wide)
     static constexpr int bytes = rec + sv + rsb + pos + 8 * (BI + 1);
-    static_assert(rec >= 8 * BI * 6, "the row accumulator reuses the element records");
+    static_assert(rec >= 8 * (BI * 6 + BI * 6 / 16 + 1), "the skewed row accumulator reuses the records");
     static_assert(rec % 16 == 0 && sv % 16 == 0, "alignment of the shared-memory carve-up");
 };
 
@@ -412,6 +414,10 @@ struct SharedLayout {
 // A2: one thread per incidence forms its element row from the record; B: one thread per
 // CSR row adds its incidences in ascending element order, as k_rowblock does, so the
 // bits are the same.
+// Row-accumulator address of the block's i-th nonzero: one pad word per 16, so row
+// threads (rows ~16 nonzeros apart) adding at the same in-row position hit different banks.
+__device__ __forceinline__ int skew(int i) { return i + (i >> 4); }
+
 // Staging tables of a block (STAGED kernels): node ids, edge dofs, element records.
 struct StageArgs {
     const int32_t *cnt, *off, *node, *edge;
@@ -422,7 +428,7 @@ template <int BI, int MAXE, int MINB, bool CALCJ, bool Q4, bool WIDE, bool STAGE
 __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const int32_t *__restrict__ blk_nelem,
                                                               const int32_t *__restrict__ blk_k0,
                                                               const int32_t *__restrict__ blk_elem,
-                                                              const uint16_t *__restrict__ inc_slot,
+                                                              const uint32_t *__restrict__ inc_sorted,
                                                               StageArgs G) {
     using L = SharedLayout<BI, MAXE>;
     static_assert(!STAGED || L::sv >= 32 * kStageMaxNodes + 8 * kStageMaxEdges, "staging area");
@@ -440,7 +446,9 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const in
     const int k0 = blk_k0[blockIdx.x], ninc = blk_k0[blockIdx.x + 1] - k0;
     const int nel = blk_nelem[blockIdx.x];
     const int nrows = a1 - a0;
-    const unsigned my_slot = tid < ninc ? inc_slot[k0 + tid] : 0u;
+    // phase A2 walks the incidences in element order (consecutive threads read the same or
+    // neighbouring records); each writes its values at its row-order position
+    const unsigned my_inc = tid < ninc ? __ldg(inc_sorted + k0 + tid) : 0u;
     if (CALCJ && tid < ninc) {
         if (WIDE) {
             spos[2 * tid] = __ldg(A.rp.inc_pos + 2 * (int64_t)(k0 + tid));
@@ -521,10 +529,9 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const in
     const int base = s_rp[0], span = s_rp[nrows] - base;
     // phase A2: one thread per incidence, the element's row from its record
     if (tid < ninc) {
-        const unsigned sl = my_slot;
-        const ElemRec &R = rec[sl & 0xFF];
-        const int loc = (int)(sl >> 8);
-        const unsigned sb = rsb[sl & 0xFF];
+        const ElemRec &R = rec[my_inc & 0xFF];
+        const int loc = (int)((my_inc >> 8) & 0xFF);
+        const unsigned sb = rsb[my_inc & 0xFF];
         Geo g;
 #pragma unroll
         for (int r = 0; r < 3; r++)
@@ -541,7 +548,7 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const in
         double bl = R.b[0];
 #pragma unroll
         for (int j = 1; j < 6; j++) bl = loc == j ? R.b[j] : bl;
-        double *out = sv + tid * kSv2;
+        double *out = sv + (my_inc >> 16) * kSv2;
         out[6] = flip(qsum_w<Q4>(nu * bl, A.qp, w0, R.adet), si);
         if (CALCJ) {
             if (R.g2 == 0.0) {
@@ -559,7 +566,7 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const in
     }
     __syncthreads();  // the records are dead from here on; sacc reuses their memory
     if (CALCJ) {
-        for (int i = tid; i < span; i += BI) sacc[i] = 0.0;
+        for (int i = tid; i < span; i += BI) sacc[skew(i)] = 0.0;
         __syncthreads();
     }
     // phase B: one thread per row adds its incidences in ascending element order
@@ -574,14 +581,14 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const in
 #pragma unroll
                     for (int j = 0; j < 6; j++) {
                         uint32_t p = (pw >> (5 * j)) & 31u;
-                        if (p != (uint32_t)kCompactMaxRow) sacc[off + p] = sacc[off + p] + v[j];
+                        if (p != (uint32_t)kCompactMaxRow) sacc[skew(off + p)] = sacc[skew(off + p)] + v[j];
                     }
                 } else {
                     uint32_t w0 = spos[2 * (k - k0)], w1 = spos[2 * (k - k0) + 1];
 #pragma unroll
                     for (int j = 0; j < 6; j++) {
                         uint32_t p = (j < 4 ? (w0 >> (8 * j)) : (w1 >> (8 * (j - 4)))) & 255u;
-                        if (p != (uint32_t)kWideMaxRow) sacc[off + p] = sacc[off + p] + v[j];
+                        if (p != (uint32_t)kWideMaxRow) sacc[skew(off + p)] = sacc[skew(off + p)] + v[j];
                     }
                 }
             }
@@ -591,7 +598,7 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const in
     }
     if (CALCJ) {
         __syncthreads();
-        for (int i = tid; i < span; i += BI) A.vals[base + i] = sacc[i];
+        for (int i = tid; i < span; i += BI) A.vals[base + i] = sacc[skew(i)];
     }
 }
 
@@ -680,7 +687,8 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
     with_shared = with_shared && (block_inc == kSharedBlockInc || block_inc == kBlockInc);
     if (with_shared) {
         if (cudaMalloc(&out->blk_elem, (size_t)(ninc > 0 ? ninc : 1) * 4) != cudaSuccess ||
-            cudaMalloc(&out->inc_slot, (size_t)(ninc > 0 ? ninc : 1) * 2) != cudaSuccess)
+            cudaMalloc(&out->inc_slot, (size_t)(ninc > 0 ? ninc : 1) * 2) != cudaSuccess ||
+            cudaMalloc(&out->inc_sorted, (size_t)(ninc > 0 ? ninc : 1) * 4) != cudaSuccess)
             with_shared = false;
     }
     // Upload the blocks; for the shared-element lists, split any block whose distinct
@@ -703,10 +711,12 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
         }
         if (block_inc == kSharedBlockInc)
             k_block_elems<kSharedBlockInc, kSharedMaxElems><<<out->nblocks, kSharedBlockInc, 0, s>>>(
-                rp, out->block_row, out->blk_nelem, out->blk_k0, out->blk_elem, out->inc_slot, nullptr);
+                rp, out->block_row, out->blk_nelem, out->blk_k0, out->blk_elem, out->inc_slot, out->inc_sorted,
+                nullptr);
         else
             k_block_elems<kBlockInc, kMaxBlockElems><<<out->nblocks, kBlockInc, 0, s>>>(
-                rp, out->block_row, out->blk_nelem, out->blk_k0, out->blk_elem, out->inc_slot, nullptr);
+                rp, out->block_row, out->blk_nelem, out->blk_k0, out->blk_elem, out->inc_slot, out->inc_sorted,
+                nullptr);
         std::vector<int32_t> nel((size_t)out->nblocks);
         if (cudaMemcpyAsync(nel.data(), out->blk_nelem, nel.size() * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) {
@@ -761,13 +771,15 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
     out->bytes = (int64_t)starts.size() * 4;
     if (out->shared_ok && stage_mesh) build_stage(*stage_mesh, out, s);
     if (out->shared_ok) {
-        out->bytes += (int64_t)out->nblocks * 8 + ninc * 6;
+        out->bytes += (int64_t)out->nblocks * 8 + ninc * 10;
     } else {
         cudaGetLastError();
         if (out->blk_nelem) cudaFree(out->blk_nelem);
         if (out->blk_k0) cudaFree(out->blk_k0);
         if (out->blk_elem) cudaFree(out->blk_elem);
         if (out->inc_slot) cudaFree(out->inc_slot);
+        if (out->inc_sorted) cudaFree(out->inc_sorted);
+        out->inc_sorted = nullptr;
         out->blk_nelem = nullptr;
         out->blk_k0 = nullptr;
         out->blk_elem = nullptr;
@@ -783,6 +795,7 @@ void free_rowblock_plan(RowBlockPlan *p) {
     if (p->blk_k0) cudaFree(p->blk_k0);
     if (p->blk_elem) cudaFree(p->blk_elem);
     if (p->inc_slot) cudaFree(p->inc_slot);
+    if (p->inc_sorted) cudaFree(p->inc_sorted);
     *p = RowBlockPlan{};
 }
 
@@ -835,7 +848,7 @@ int launch_rowblock_shared_jacobian(const RowBlockPlan &bp, const ElemData &m, c
                            : k_rowblock_shared<BI_, ME_, MB_, CJ, Q, W, false>;                          \
         const int sm = SharedLayout<BI_, ME_>::bytes;                                                    \
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                     \
-        kern<<<bp.nblocks, BI_, sm, s>>>(A, bp.blk_nelem, bp.blk_k0, bp.blk_elem, bp.inc_slot, G);       \
+        kern<<<bp.nblocks, BI_, sm, s>>>(A, bp.blk_nelem, bp.blk_k0, bp.blk_elem, bp.inc_sorted, G);     \
     } while (0)
 #define MAG_RS_ALL(BI_, ME_, MB_)                                                                         \
     do {                                                                                                 \

@@ -27,6 +27,7 @@ struct RowBlockPlan {
     int32_t *blk_k0 = nullptr;     // [nblocks+1] first incidence of each block
     int32_t *blk_elem = nullptr;   // [ninc] (first blk_nelem[b] entries after the block's offset)
     uint16_t *inc_slot = nullptr;  // [ninc] slot | local row << 8
+    uint32_t *inc_sorted = nullptr; // [ninc] per block in element order: slot | local row << 8 | incidence << 16
     int shared_ok = 0;
     // staging: per block its distinct nodes and edge dofs, and per distinct element a
     // record of local node / edge indices, tag and sign bits (exact offsets per block)
