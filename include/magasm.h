@@ -137,6 +137,20 @@ int mag_assemble_jacobian(mag_mesh *mesh, const double *d_sol, double *d_vals, d
  * (assemble_curl_curl_kernel_mex.cpp:18-121 + Assembler.m:37-38). */
 int mag_assemble_stiffness(mag_mesh *mesh, const double *d_nu, double *d_vals, void *stream);
 
+/* Harmonic-balance assembly (assemble_hbfem_kernel_mex.cpp:26-258, called through
+ * Assembler.assembleHBFEM by HBFEMSolver.m:78,96; that wrapper is absent from the
+ * reference). Harmonic field d_sol_re/d_sol_im [K][num_dofs] (= MATLAB's [Ndof x K]
+ * column-major; imaginary part may be NULL), AFT matrices D [K][N] (D(t,h) at
+ * h*N + t) and P [N][K] (P(h,t) at t*K + h), imaginary parts may be NULL. Writes
+ * the harmonic residual d_res_re/d_res_im [K][num_dofs] (the gateway's R triplets
+ * summed as sparse() does) and, when d_vals is not NULL, the DC-reluctivity block
+ * on the CSR pattern; harmonic k's Jacobian block is Scalings[k] * d_vals. The
+ * spline coefficient offsets come from mag_mesh_set_materials (the gateway never
+ * sets them, so it is defined only for linear materials). K <= 16. */
+int mag_assemble_hbfem(mag_mesh *mesh, const double *d_sol_re, const double *d_sol_im, int K,
+                       const double *d_d_re, const double *d_d_im, const double *d_p_re, const double *d_p_im,
+                       int N, double *d_vals, double *d_res_re, double *d_res_im, void *stream);
+
 /* Newton residual at d_sol with the tangent evaluated at a seeded state: per
  * element the flux density B of d_sol scaled by d_bscale[e] (the learned warm
  * start's first Jacobian; no counterpart in the reference). Same outputs as

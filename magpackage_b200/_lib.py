@@ -56,6 +56,7 @@ _PROTOS = {
     "mag_assemble_source": ([_vp, _vp, _vp, _vp], _int),
     "mag_element_b": ([_vp, _vp, _vp, _vp, _vp], _int),
     "mag_element_nu": ([_vp, _vp, _vp, _vp, _vp], _int),
+    "mag_assemble_hbfem": ([_vp, _vp, _vp, _int, _vp, _vp, _vp, _vp, _int, _vp, _vp, _vp, _vp], _int),
     "mag_assemble_jacobian_seeded": ([_vp, _vp, _vp, _vp, _vp, _vp], _int),
     "mag_seed_midpoint": ([_vp, _vp, _vp, _vp, _vp], _int),
     "mag_csr_spmv": ([_i64, _vp, _vp, _vp, _vp, _vp, _vp], _int),

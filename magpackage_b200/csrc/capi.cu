@@ -12,6 +12,7 @@
 #include "internal.h"
 #include "mlp.cuh"
 #include "sparse.cuh"
+#include "hbfem.cuh"
 
 namespace mag {
 
@@ -600,6 +601,31 @@ int mag_assemble_jacobian_seeded(mag_mesh *m, const double *d_sol, const double 
     cudaStream_t s = (cudaStream_t)stream;
     MAG_TRY(launch_jacobian_seeded_elems(m->elems(), d_sol, d_bscale, m->qp, m->mat.mp, m->scratch, s));
     MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, d_vals, d_res, s));
+    return finish(s);
+}
+
+int mag_assemble_hbfem(mag_mesh *m, const double *d_sol_re, const double *d_sol_im, int K, const double *d_d_re,
+                       const double *d_d_im, const double *d_p_re, const double *d_p_im, int N, double *d_vals,
+                       double *d_res_re, double *d_res_im, void *stream) {
+    MAG_TRY(require_ready(m, true));
+    if (!d_sol_re || !d_d_re || !d_p_re || !d_res_re || !d_res_im || K < 1 || N < 1) {
+        set_error("mag_assemble_hbfem: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (K > kMaxHarm) {
+        set_error("mag_assemble_hbfem: %d harmonics (at most %d per call)", K, kMaxHarm);
+        return MAG_E_UNSUPPORTED;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    double *rscr = nullptr;
+    MAG_CUDA_TRY(cudaMallocAsync((void **)&rscr, (size_t)m->ne * 6 * 2 * K * sizeof(double), s));
+    int rc = launch_hbfem(m->elems(), m->rows(), m->pat.max_row, d_sol_re, d_sol_im, K, d_d_re, d_d_im, d_p_re,
+                          d_p_im, N, m->qp, m->mat.mp, m->scratch, rscr, d_vals, d_res_re, d_res_im, s);
+    cudaFreeAsync(rscr, s);
+    if (rc != MAG_OK) {
+        set_error("mag_assemble_hbfem: launch failed (%s)", cudaGetErrorString(cudaGetLastError()));
+        return rc;
+    }
     return finish(s);
 }
 

@@ -66,6 +66,13 @@ class MexInputs:
         return self.P.shape[0]
 
 
+def _split(a):
+    """Column-major real and imaginary parts of a 2-D array; None for a real array."""
+    a = np.asarray(a)
+    re = _f64(np.real(a).T.ravel())
+    return re, (_f64(np.imag(a).T.ravel()) if np.iscomplexobj(a) else None)
+
+
 def mex_inputs(P, T0, t2e0, sign, tags) -> MexInputs:
     """Convert 0-based int mesh arrays to the reference's double/1-based layout."""
     return MexInputs(P=_f64(P), T=_f64(np.asarray(T0) + 1), Dofs=_f64(np.asarray(t2e0) + 1),
@@ -151,6 +158,27 @@ class Port(_Lib):
                                _d(qw), C.c_int(qw.size), _d(val), _d(I), _d(V))
         return I, V
 
+    def hbfem(self, m: MexInputs, sol, D, P, qw, curl, packed, calc_j=True, scalings=None):
+        """assemble_hbfem_kernel_mex restated with the coefficient offsets passed.
+
+        sol: complex [Ndof, K]; D: complex [N, K]; P: complex [K, N]. Returns
+        (I, J, V, R_rows, R_cols, R_re, R_im) in the gateway's layout."""
+        ne, (ndof, K), N = m.ne, sol.shape, D.shape[0]
+        sr, si = _split(sol)  # column-major [Ndof x K]; a real input has no imaginary part
+        dr, di = _split(D)    # [N x K]
+        pr, pi = _split(P)    # [K x N]
+        sc = _f64(np.ones(K) if scalings is None else scalings)
+        pk = [_f64(a) for a in packed.as_tuple()]
+        qw, curl = _f64(qw), _f64(curl)
+        nK = 36 * K * ne if calc_j else 0
+        I, J, V = (np.zeros(max(nK, 1)) for _ in range(3))
+        Rr, Rc, Rre, Rim = (np.zeros(6 * K * ne) for _ in range(4))
+        self.lib.oracle_hbfem(_d(m.P), _d(m.T), C.c_int64(ne), _d(m.Dofs), _d(m.Signs), _d(m.Tags), _d(sr),
+                              _d(si), C.c_int64(ndof), C.c_int(K), _d(dr), _d(di), _d(pr), _d(pi), C.c_int(N),
+                              _d(qw), C.c_int(qw.size), _d(curl), *[_d(a) for a in pk], C.c_int(int(calc_j)),
+                              _d(sc), _d(I), _d(J), _d(V), _d(Rr), _d(Rc), _d(Rre), _d(Rim))
+        return I[:nK], J[:nK], V[:nK], Rr, Rc, Rre, Rim
+
     def sparse_csr(self, I, J, V, N, drop_zeros=True):
         I, J, V = _f64(I), _f64(J), _f64(V)
         n = I.size
@@ -188,7 +216,7 @@ class RefMex(_Lib):
     def __init__(self, path: str = REF_SO):
         super().__init__(path)
         L = self.lib
-        for f in ("ref_jacobian", "ref_curl_curl", "ref_mass", "ref_source"):
+        for f in ("ref_jacobian", "ref_curl_curl", "ref_mass", "ref_source", "ref_hbfem"):
             getattr(L, f).restype = C.c_int
         L.ref_last_error.restype = C.c_char_p
         self.last_seconds = 0.0
@@ -253,6 +281,34 @@ class RefMex(_Lib):
         self._check(rc)
         self.last_seconds = secs.value
         return I, V
+
+
+    def hbfem(self, m: MexInputs, sol, D, P, qw, curl, packed, calc_j=True, scalings=None):
+        """The reference gateway (22 inputs). It leaves the spline coefficient offsets unset,
+        so only linear materials are defined; the caller must not pass nonlinear ones."""
+        ne, (ndof, K), N = m.ne, sol.shape, D.shape[0]
+        if np.any(np.asarray(packed.is_non) != 0):
+            raise ValueError("the reference HBFEM gateway is undefined for nonlinear materials")
+        sr, si = _split(sol)
+        dr, di = _split(D)
+        pr, pi = _split(P)
+        sc = _f64(np.ones(K) if scalings is None else scalings)
+        pk = [_f64(a) for a in packed.as_tuple()]
+        qw, curl = _f64(qw), _f64(curl)
+        nK = 36 * K * ne if calc_j else 0
+        I, J, V = (np.zeros(max(nK, 1)) for _ in range(3))
+        Rr, Rc, Rre, Rim = (np.zeros(6 * K * ne) for _ in range(4))
+        secs = C.c_double(0)
+        nmat = pk[0].size
+        z = C.c_size_t
+        rc = self.lib.ref_hbfem(
+            _d(m.P), z(m.nn), _d(m.T), z(ne), _d(m.Dofs), _d(m.Signs), _d(m.Tags), _d(sr), _d(si), z(ndof), z(K),
+            _d(dr), _d(di), _d(pr), _d(pi), z(N), _d(qw), z(qw.size), _d(curl), _d(pk[0]), _d(pk[1]), _d(pk[2]),
+            z(nmat), _d(pk[3]), z(pk[3].size), _d(pk[4]), z(pk[4].size), _d(pk[5]), _d(pk[6]),
+            C.c_int(int(calc_j)), _d(sc), _d(I), _d(J), _d(V), _d(Rr), _d(Rc), _d(Rre), _d(Rim), C.byref(secs))
+        self._check(rc)
+        self.last_seconds = secs.value
+        return I[:nK], J[:nK], V[:nK], Rr, Rc, Rre, Rim
 
 
 def ref_available() -> bool:

@@ -16,6 +16,7 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <stdlib.h>
 
 typedef struct {
     double g[3][3]; /* g[r][c]: row r (x,y,z), column c (edge vector c) */
@@ -294,5 +295,116 @@ void oracle_source(const double *P, const double *T, int64_t Ne, const double *D
             I[6 * e + i] = (double)(int64_t)Dofs[6 * e + i];
             V[6 * e + i] = f[i] * Signs[6 * e + i];
         }
+    }
+}
+
+/* Harmonic-balance element kernel, restating src/mex/assemble_hbfem_kernel_mex.cpp:26-258
+ * with the coefficient offsets passed (the gateway leaves them unset). For each element:
+ * the signed harmonic edge values A_h (re, im), the time samples
+ * A(t) = sum_h (Re A_h Re D(t,h) - Im A_h Im D(t,h)), per quadrature point the curls,
+ * per time sample B(t), nu(|B(t)|^2), H = nu B, and the harmonic residual
+ * R_h += w (C_i . H) P(h,t) (re, im); the Jacobian block is w nu_dc C_r . C_c with nu_dc
+ * the time average of nu, repeated per harmonic and scaled by Scalings[h]. */
+void oracle_hbfem(const double *P, const double *T, int64_t Ne, const double *Dofs,
+                  const double *Signs, const double *Tags, const double *SolR, const double *SolI,
+                  int64_t Ndof, int K, const double *DR, const double *DI, const double *PR,
+                  const double *PI, int N, const double *Qw, int nq, const double *CurlRef,
+                  const double *lin, const double *isNon, const double *maxB, const double *brk,
+                  const double *coe, const double *start, const double *cnt, const double *coeStart,
+                  int calcJ, const double *Scalings, double *I, double *J, double *V, double *Rrows,
+                  double *Rcols, double *Rre, double *Rim) {
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < Ne; e++) {
+        double *ar = malloc(sizeof(double) * 6 * K), *ai = malloc(sizeof(double) * 6 * K);
+        double *at = malloc(sizeof(double) * 6 * N);
+        double *rr = calloc((size_t)6 * K, sizeof(double)), *ri = calloc((size_t)6 * K, sizeof(double));
+        double kb[36] = {0};
+        double d[6], s[6];
+        for (int k = 0; k < 6; k++) {
+            d[k] = Dofs[6 * e + k];
+            s[k] = Signs[6 * e + k];
+            int64_t g = (int64_t)d[k] - 1;
+            for (int h = 0; h < K; h++) {
+                ar[k + 6 * h] = SolR[g + h * Ndof] * s[k];
+                ai[k + 6 * h] = SolI ? SolI[g + h * Ndof] * s[k] : 0.0;
+            }
+        }
+        for (int t = 0; t < N; t++)
+            for (int k = 0; k < 6; k++) {
+                double acc = 0.0;
+                for (int h = 0; h < K; h++) {
+                    double term = ar[k + 6 * h] * DR[t + h * N];
+                    if (SolI && DI) term -= ai[k + 6 * h] * DI[t + h * N];
+                    acc += term;
+                }
+                at[k + 6 * t] = acc;
+            }
+        double v[4][3];
+        gather_vertices(P, T, e, v);
+        mat3 Jm;
+        double det = edge_matrix(v, &Jm);
+        double rdet = 1.0 / det, adet = fabs(det);
+        int tag = (int)Tags[e];
+        for (int q = 0; q < nq; q++) {
+            double w = Qw[q] * adet;
+            double C[6][3];
+            for (int i = 0; i < 6; i++) {
+                double c[3];
+                ref_vec(CurlRef, i, q, c);
+                double y[3];
+                apply(&Jm, c, y);
+                for (int r = 0; r < 3; r++) C[i][r] = y[r] * rdet;
+            }
+            double sum_nu = 0.0;
+            for (int t = 0; t < N; t++) {
+                double B[3] = {0.0, 0.0, 0.0};
+                for (int i = 0; i < 6; i++)
+                    for (int r = 0; r < 3; r++) B[r] += C[i][r] * at[i + 6 * t];
+                double bsq = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+                double nu, dnu;
+                material_eval(bsq, tag, lin, isNon, maxB, brk, coe, start, cnt, coeStart, &nu, &dnu);
+                sum_nu += nu;
+                double H[3] = {nu * B[0], nu * B[1], nu * B[2]};
+                for (int h = 0; h < K; h++) {
+                    double pr = PR[h + t * K];
+                    for (int i = 0; i < 6; i++) {
+                        double dot = C[i][0] * H[0] + C[i][1] * H[1] + C[i][2] * H[2];
+                        rr[i + 6 * h] += w * dot * pr;
+                        if (PI) ri[i + 6 * h] += w * dot * PI[h + t * K];
+                    }
+                }
+            }
+            if (calcJ) {
+                double nu_dc = sum_nu / N;
+                for (int c = 0; c < 6; c++)
+                    for (int r = 0; r < 6; r++) {
+                        double dot = C[r][0] * C[c][0] + C[r][1] * C[c][1] + C[r][2] * C[c][2];
+                        kb[r + 6 * c] += w * nu_dc * dot;
+                    }
+            }
+        }
+        int64_t oR = e * 6 * K;
+        for (int h = 0, n = 0; h < K; h++)
+            for (int k = 0; k < 6; k++, n++) {
+                Rrows[oR + n] = d[k];
+                Rcols[oR + n] = (double)(h + 1);
+                Rre[oR + n] = rr[k + 6 * h] * s[k];
+                Rim[oR + n] = ri[k + 6 * h] * s[k];
+            }
+        if (calcJ) {
+            int64_t oK = e * 36 * K;
+            for (int h = 0, n = 0; h < K; h++)
+                for (int c = 0; c < 6; c++)
+                    for (int r = 0; r < 6; r++, n++) {
+                        I[oK + n] = d[r] + (double)h * (double)Ndof;
+                        J[oK + n] = d[c] + (double)h * (double)Ndof;
+                        V[oK + n] = kb[r + 6 * c] * Scalings[h] * s[r] * s[c];
+                    }
+        }
+        free(ar);
+        free(ai);
+        free(at);
+        free(rr);
+        free(ri);
     }
 }

@@ -56,6 +56,19 @@ void oracle_source(const double *P, const double *T, int64_t Ne, const double *D
                    const double *Signs, const double *Js, const double *Qw, int nq,
                    const double *ValRef, double *I, double *V);
 
+/* Harmonic-balance element kernel, src/mex/assemble_hbfem_kernel_mex.cpp:26-258, with the
+ * spline coefficient offsets coeStart passed (the gateway leaves them unset). SolR/SolI
+ * [Ndof x K], DR/DI [N x K], PR/PI [K x N] column-major; SolI, DI, PI may be NULL.
+ * Outputs as the gateway: I,J,V [36 K Ne] (when calcJ), R rows/cols/re/im [6 K Ne]. */
+void oracle_hbfem(const double *P, const double *T, int64_t Ne, const double *Dofs,
+                  const double *Signs, const double *Tags, const double *SolR, const double *SolI,
+                  int64_t Ndof, int K, const double *DR, const double *DI, const double *PR,
+                  const double *PI, int N, const double *Qw, int nq, const double *CurlRef,
+                  const double *lin, const double *isNon, const double *maxB, const double *brk,
+                  const double *coe, const double *start, const double *cnt, const double *coeStart,
+                  int calcJ, const double *Scalings, double *I, double *J, double *V, double *Rrows,
+                  double *Rcols, double *Rre, double *Rim);
+
 /* MATLAB sparse(I(valid),J(valid),V(valid),N,N) as used at Assembler.m:37-38,
  * 205-206: valid = I>0 & J>0; duplicates summed in order of appearance;
  * drop_zeros != 0 removes entries whose sum is exactly zero (MATLAB stores no

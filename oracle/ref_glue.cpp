@@ -73,6 +73,7 @@ void ref_jacobian_mexFunction(int, mxArray *[], int, const mxArray *[]);
 void ref_curl_curl_mexFunction(int, mxArray *[], int, const mxArray *[]);
 void ref_mass_mexFunction(int, mxArray *[], int, const mxArray *[]);
 void ref_source_mexFunction(int, mxArray *[], int, const mxArray *[]);
+void ref_hbfem_mexFunction(int, mxArray *[], int, const mxArray *[]);
 
 const char *ref_last_error(void) { return g_err_msg; }
 
@@ -180,6 +181,34 @@ int ref_source(const double *P, size_t Nn, const double *T, size_t Ne, const dou
     double *outs[2] = {I, V};
     size_t outn[2] = {Ne * 6, Ne * 6};
     return run(ref_source_mexFunction, 2, 7, in, outs, outn, seconds);
+}
+
+/* [I,J,V,R_rows,R_cols,R_re,R_im] = assemble_hbfem_kernel_mex(22 args)
+ * (assemble_hbfem_kernel_mex.cpp:26-57). SolR/SolI [Ndof x K], DR/DI [N x K],
+ * PR/PI [K x N] column-major; a NULL imaginary part is passed as an empty array.
+ * The gateway reads seven material arrays and leaves the coefficient offsets
+ * unset, so only linear materials give defined results. */
+int ref_hbfem(const double *P, size_t Nn, const double *T, size_t Ne, const double *Dofs,
+              const double *Signs, const double *Tags, const double *SolR, const double *SolI, size_t Ndof,
+              size_t K, const double *DR, const double *DI, const double *PR, const double *PI, size_t N,
+              const double *Qw, size_t nq, const double *CurlRef, const double *lin, const double *isNon,
+              const double *maxB, size_t nmat, const double *brk, size_t nbrk, const double *coe, size_t ncoe,
+              const double *start, const double *cnt, int calcJ, const double *Scalings, double *I, double *J,
+              double *V, double *Rrows, double *Rcols, double *Rre, double *Rim, double *seconds) {
+    double cj = calcJ ? 1.0 : 0.0;
+    mxArray in[22] = {
+        wrap(P, 3, Nn),          wrap(T, 4, Ne),          wrap(Dofs, 6, Ne),      wrap(Signs, 6, Ne),
+        wrap(Tags, 1, Ne),       wrap(SolR, Ndof, K),     wrap(SolI, SolI ? Ndof : 0, SolI ? K : 0),
+        wrap(DR, N, K),          wrap(DI, DI ? N : 0, DI ? K : 0),
+        wrap(PR, K, N),          wrap(PI, PI ? K : 0, PI ? N : 0),
+        wrap(Qw, 1, nq),         wrap(CurlRef, 18, nq),
+        wrap(lin, nmat, 1),      wrap(isNon, nmat, 1),    wrap(maxB, nmat, 1),    wrap(brk, nbrk, 1),
+        wrap(coe, ncoe, 1),      wrap(start, nmat, 1),    wrap(cnt, nmat, 1),     wrap(&cj, 1, 1),
+        wrap(Scalings, K, 1)};
+    size_t nK = calcJ ? Ne * 36 * K : 0, nR = Ne * 6 * K;
+    double *outs[7] = {I, J, V, Rrows, Rcols, Rre, Rim};
+    size_t outn[7] = {nK, nK, nK, nR, nR, nR, nR};
+    return run(ref_hbfem_mexFunction, 7, 22, in, outs, outn, seconds);
 }
 
 }  // extern "C"

@@ -144,3 +144,53 @@ def test_port_matches_live_reference(oracle_port, oracle_ref):
     assert bits_equal(oracle_ref.mass(m, sig, qw, val)[2], oracle_port.mass(m, sig, qw, val)[2])
     js = np.random.default_rng(5).normal(size=(mesh.num_elements, 3))
     assert bits_equal(oracle_ref.source(m, js, qw, val)[1], oracle_port.source(m, js, qw, val)[1])
+
+
+def _hbfem_case(oracle_port, iron_nonlinear, n=(4, 3, 3), seed=11, harmonics=(0, 1, 3), imag=True):
+    from magpackage_b200.hbfem import AFT
+
+    mesh = synth.kuhn_box(*n, seed=seed)
+    tags = synth.cube_layout(mesh)
+    edges, t2e, sign = oracle_port.generate_edges(mesh.T)
+    m = mex_inputs(mesh.P, mesh.T, t2e, sign, tags)
+    qw, val, curl = quadrature.reference_data(2)
+    pk = material.pack_material_data(synth.standard_materials(iron_nonlinear))
+    aft = AFT(harmonics)
+    rng = np.random.default_rng(seed)
+    E, K = edges.shape[0], len(harmonics)
+    sol = rng.normal(0, 0.05, (E, K)) + (1j * rng.normal(0, 0.05, (E, K)) if imag else 0.0)
+    return mesh, m, qw, curl, pk, aft, sol
+
+
+@pytest.mark.parametrize("imag", [True, False])
+def test_hbfem_port_matches_reference_on_linear_materials(oracle_port, oracle_ref, imag):
+    """assemble_hbfem_kernel_mex compiled unchanged (defined for linear materials only:
+    it leaves the spline coefficient offsets unset) against the restatement, bit for bit."""
+    mesh, m, qw, curl, pk, aft, sol = _hbfem_case(oracle_port, False, imag=imag)
+    D = aft.D if imag else np.real(aft.D)
+    P = aft.P if imag else np.real(aft.P)
+    sc = np.array([1.0, 2.5, -0.75])
+    for cj in (True, False):
+        r = oracle_ref.hbfem(m, sol, D, P, qw, curl, pk, cj, sc)
+        p = oracle_port.hbfem(m, sol, D, P, qw, curl, pk, cj, sc)
+        assert all(bits_equal(x, y) for x, y in zip(r, p))
+        assert np.abs(p[5]).max() > 0
+
+
+def test_hbfem_single_dc_harmonic_is_the_static_residual(oracle_port):
+    """With the harmonic set {0} and one time sample (D = P = 1) the harmonic-balance
+    residual is the static Newton residual of the Jacobian kernel on nonlinear iron (the
+    two kernels order the same products differently, so they agree to rounding)."""
+    from magpackage_b200.hbfem import AFT
+
+    mesh, m, qw, curl, pk, _, sol = _hbfem_case(oracle_port, True, harmonics=(0,), imag=False)
+    aft = AFT([0], n_time_steps=1)
+    assert aft.D.shape == (1, 1) and aft.P[0, 0] == 1.0
+    E = sol.shape[0]
+    x = np.real(sol[:, 0]) * 40.0  # drive the iron through the spline's interior and knee
+    _, _, _, Rr, Rc, Rre, Rim = oracle_port.hbfem(m, x[:, None], aft.D, aft.P, qw, curl, pk, False)
+    hb = oracle_port.sparse_vec(Rr, Rre, E)
+    _, _, _, Ri, Rv = oracle_port.jacobian(m, x, qw, curl, pk, False)
+    st = oracle_port.sparse_vec(Ri, Rv, E)
+    assert np.abs(hb - st).max() <= 1e-13 * np.abs(st).max()
+    assert np.all(Rim == 0.0)
