@@ -56,7 +56,7 @@ typedef struct {
     int32_t fused_grid;     /* co-resident CTAs of that launch */
     int64_t device_bytes;   /* memory held by the handle */
     int32_t shared_blocks;  /* row blocks of MAG_SCHEDULE_SHARED_ROW_BLOCKS (0 = not available) */
-    int32_t shared_staged;  /* 1 if those blocks stage their nodes and edge values in shared memory */
+    int32_t shared_staged;  /* 1 once MAG_SCHEDULE_STAGED_ROW_BLOCKS has been selected (tables built) */
 } mag_mesh_info;
 
 /* Jacobian assembly schedules; all give identical bits. */
@@ -67,7 +67,8 @@ typedef struct {
 #define MAG_SCHEDULE_SHARED_ROW_BLOCKS 3 /* as 2, each block's distinct elements evaluated once in shared
                                             memory (default; standard curl table, else runs as 2) */
 #define MAG_SCHEDULE_STAGED_ROW_BLOCKS 4 /* as 3, the block's distinct nodes and edge values first gathered
-                                            once into shared memory (measured slower than 3 on B200) */
+                                            once into shared memory (measured slower than 3 on B200); its
+                                            tables are built when it is first selected */
 
 /* ---- library ------------------------------------------------------------ */
 

@@ -459,8 +459,7 @@ int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t N
         free_rowblock_plan(&m->rowblock);
         cudaGetLastError();
     }
-    const ElemData ed = m->elems();
-    if (build_rowblock_plan(m->rows(), &m->rowshared, s, kSharedBlockInc, true, &ed) == MAG_OK &&
+    if (build_rowblock_plan(m->rows(), &m->rowshared, s, kSharedBlockInc, true) == MAG_OK &&
         m->rowshared.shared_ok) {
         m->bytes += m->rowshared.bytes;
     } else {
@@ -704,6 +703,20 @@ int mag_mesh_set_option(mag_mesh *m, int option, int64_t value) {
         return MAG_E_ARG;
     }
     if (option == MAG_OPTION_SCHEDULE) {
+        if (value == MAG_SCHEDULE_STAGED_ROW_BLOCKS && m->rowshared.shared_ok && !m->rowshared.staged_ok) {
+            // the staging tables are built on first request (blocks re-split to their capacity)
+            RowBlockPlan staged{};
+            const ElemData ed = m->elems();
+            if (build_rowblock_plan(m->rows(), &staged, nullptr, kSharedBlockInc, true, &ed) == MAG_OK &&
+                staged.shared_ok && staged.staged_ok) {
+                m->bytes += staged.bytes - m->rowshared.bytes;
+                free_rowblock_plan(&m->rowshared);
+                m->rowshared = staged;
+            } else {
+                free_rowblock_plan(&staged);
+                cudaGetLastError();
+            }
+        }
         if ((value == MAG_SCHEDULE_L2_RING && !m->fused.ok) ||
             (value == MAG_SCHEDULE_ROW_BLOCKS && !m->rowblock.ok) ||
             (value == MAG_SCHEDULE_SHARED_ROW_BLOCKS && !m->rowshared.shared_ok) ||
