@@ -251,6 +251,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Each rank's device times -> the element-wise maximum over ranks (every rank gets it)."""
+    import torch
+
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def whole_job_rate(world, units_per_rank, ms):
+    """Units all ranks processed per second, in millions, at the slowest rank's time."""
+    return world * units_per_rank / (ms * 1e-3) / 1e6
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -464,10 +479,7 @@ def main():
     plan.check()
     clk = clocks.stop()
 
-    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -481,7 +493,7 @@ def main():
         b_elem = algorithmic_bytes_per_elem(ne, mesh.num_nodes, E, nnz)
         peak, peak_kind = measured_peak()
         achieved = b_elem * ne / (ms_asm * 1e-3) / 1e9
-        value = world * ne / (ms * 1e-3) / 1e6
+        value = whole_job_rate(world, ne, ms)
         out = {
             "metric": "Jacobian assembly Melem/s (FP64 CSR)", "value": value, "unit": "Melem/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -508,7 +520,7 @@ def main():
                          "peak_source": peak_kind, "bytes_per_elem": b_elem,
                          "scope": "whole assembly" + (" (one kernel)" if single else
                                                       " (element kernel + row reduction)")},
-            "e2e": {"value": world * ne / (e2e_ms * 1e-3) / 1e6, "unit": "Melem/s",
+            "e2e": {"value": whole_job_rate(world, ne, e2e_ms), "unit": "Melem/s",
                     "h2d_bytes_per_step": 8 * E, "d2h_bytes_per_step": 8 * (nnz + E)},
             "gpu_launches": ((1 if single else 2) + (1 if with_mlp else 0)) * args.steps,
             "clocks": clk,
