@@ -163,10 +163,11 @@ int mag_assemble_jacobian_seeded(mag_mesh *mesh, const double *d_sol, const doub
 /* Per-element scale of the seeded tangent: beta_e = (|B_e| + |B_hat_e|)/(2|B_e|),
  * B_e the flux density of d_sol and |B_hat_e|^2 where the element's nonlinear
  * nu(|B|^2) equals d_nu_hat[e] (a predicted reluctivity), i.e. the tangent at the
- * midpoint between the current and the predicted state. beta = 1 for linear
- * materials, d_nu_hat[e] <= 0 or B_e = 0. No counterpart in the reference. */
-int mag_seed_midpoint(mag_mesh *mesh, const double *d_sol, const double *d_nu_hat, double *d_bscale,
-                      void *stream);
+ * midpoint between the current and the predicted state, clamped to the trust region
+ * [1/max_scale, max_scale] (max_scale >= 1). beta = 1 for linear materials,
+ * d_nu_hat[e] <= 0 or B_e = 0. No counterpart in the reference. */
+int mag_seed_midpoint(mag_mesh *mesh, const double *d_sol, const double *d_nu_hat, double max_scale,
+                      double *d_bscale, void *stream);
 
 /* Sigma-weighted Nedelec mass M(sigma) (assemble_mass_kernel_mex.cpp:17-127 +
  * Assembler.m:52-53,71-72). d_sigma [Ne], or NULL for sigma = 1 (the

@@ -58,7 +58,7 @@ _PROTOS = {
     "mag_element_nu": ([_vp, _vp, _vp, _vp, _vp], _int),
     "mag_assemble_hbfem": ([_vp, _vp, _vp, _int, _vp, _vp, _vp, _vp, _int, _vp, _vp, _vp, _vp], _int),
     "mag_assemble_jacobian_seeded": ([_vp, _vp, _vp, _vp, _vp, _vp], _int),
-    "mag_seed_midpoint": ([_vp, _vp, _vp, _vp, _vp], _int),
+    "mag_seed_midpoint": ([_vp, _vp, _vp, C.c_double, _vp, _vp], _int),
     "mag_csr_spmv": ([_i64, _vp, _vp, _vp, _vp, _vp, _vp], _int),
     "mag_csr_apply_dirichlet": ([_i64, _vp, _vp, _vp, _vp, _vp, _vp], _int),
     "mag_pcg_create": ([_i64, C.POINTER(_vp)], _int),

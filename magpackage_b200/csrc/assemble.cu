@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(128) k_jacobian_seeded_elems(ElemData m, const
 // nu_hat <= 0, or B = 0.
 __global__ void __launch_bounds__(128) k_seed_midpoint(ElemData m, const double *__restrict__ sol,
                                                        const double *__restrict__ nu_hat, MaterialParams mp,
-                                                       double *__restrict__ bscale) {
+                                                       double max_scale, double *__restrict__ bscale) {
     int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
     const int tag = m.tags[e];
@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(128) k_seed_midpoint(ElemData m, const double 
                 }
             }
             beta = 0.5 * (bp + sqrt(s_hat)) / bp;
+            beta = fmin(fmax(beta, 1.0 / max_scale), max_scale);  // trust region of the seed
         }
     }
     bscale[e] = beta;
@@ -446,8 +447,8 @@ int launch_jacobian_seeded_elems(const ElemData &m, const double *sol, const dou
 }
 
 int launch_seed_midpoint(const ElemData &m, const double *sol, const double *nu_hat, const MaterialParams &mp,
-                         double *bscale, cudaStream_t s) {
-    k_seed_midpoint<<<blocks(m.ne, 128), 128, 0, s>>>(m, sol, nu_hat, mp, bscale);
+                         double max_scale, double *bscale, cudaStream_t s) {
+    k_seed_midpoint<<<blocks(m.ne, 128), 128, 0, s>>>(m, sol, nu_hat, mp, max_scale, bscale);
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
 

@@ -12,7 +12,7 @@ int launch_jacobian_elems(const ElemData &m, const double *sol, const QuadParams
 int launch_jacobian_seeded_elems(const ElemData &m, const double *sol, const double *bscale, const QuadParams &qp,
                                  const MaterialParams &mp, double *scratch, cudaStream_t s);
 int launch_seed_midpoint(const ElemData &m, const double *sol, const double *nu_hat, const MaterialParams &mp,
-                         double *bscale, cudaStream_t s);
+                         double max_scale, double *bscale, cudaStream_t s);
 int launch_stiffness_elems(const ElemData &m, const double *nu, const QuadParams &qp,
                            double *scratch, cudaStream_t s);
 int launch_mass_elems(const ElemData &m, const double *sigma, const QuadParams &qp, double *scratch,

@@ -628,9 +628,10 @@ int mag_assemble_hbfem(mag_mesh *m, const double *d_sol_re, const double *d_sol_
     return finish(s);
 }
 
-int mag_seed_midpoint(mag_mesh *m, const double *d_sol, const double *d_nu_hat, double *d_bscale, void *stream) {
+int mag_seed_midpoint(mag_mesh *m, const double *d_sol, const double *d_nu_hat, double max_scale, double *d_bscale,
+                      void *stream) {
     MAG_TRY(require_ready(m, true));
-    if (!d_sol || !d_nu_hat || !d_bscale) {
+    if (!d_sol || !d_nu_hat || !d_bscale || !(max_scale >= 1.0)) {
         set_error("mag_seed_midpoint: bad arguments");
         return MAG_E_ARG;
     }
@@ -639,7 +640,7 @@ int mag_seed_midpoint(mag_mesh *m, const double *d_sol, const double *d_nu_hat, 
         return MAG_E_UNSUPPORTED;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    MAG_TRY(launch_seed_midpoint(m->elems(), d_sol, d_nu_hat, m->mat.mp, d_bscale, s));
+    MAG_TRY(launch_seed_midpoint(m->elems(), d_sol, d_nu_hat, m->mat.mp, max_scale, d_bscale, s));
     return finish(s);
 }
 

@@ -19,11 +19,14 @@ gets stricter the better the initial guess, so it cannot compare warm starts.
 Warm starts of step t (x_0 = x_{t-1} in all modes, TransientSolver.m:159):
   plain    -- every Newton iteration uses the tangent at the current iterate;
   learned  -- the MLP predicts each nonlinear element's nu_e at the end of step t
-              from |B|_{t-1}, |B|_{t-2}, |J(t)| and the material id; inverting the
+              from |B|_{t-1}, |B|_{t-2}, |J(t)| and the material id (as the ratio
+              nu_t / nu(|B|_{t-1}), multiplied onto the exactly evaluated nu at
+              x_{t-1}, so its error scales with the step's change); inverting the
               element's B-H table turns it into a predicted |B_hat_e|, and the FIRST
               Jacobian of the step is evaluated at the midpoint state
               (|B_{t-1}| + |B_hat|)/2 (per element, along B_{t-1}) -- a secant-like
-              tangent over the step -- while its residual stays the true R(x_{t-1}).
+              tangent over the step, the scale kept in a trust region [1/1.25, 1.25] --
+              while its residual stays the true R(x_{t-1}).
               Later iterations are plain Newton to the same tolerance, so a bad
               prediction costs iterations, never accuracy;
   ideal    -- the same seeding with the converged nu of the step (a bound on what
@@ -69,6 +72,7 @@ class TransientConfig:
     reg_rel: float = 1e-5      # TransientSolver.RegScaleRel
     cg_rtol: float = 1e-10
     cg_max: int = 20000
+    seed_max_scale: float = 1.25  # trust region of the seeded tangent's flux-density scale
 
 
 @dataclass
@@ -149,6 +153,7 @@ class TransientProblem:
         jb, _ = self.plan.element_b(t_edge)
         self.j_unit = jb.contiguous()
         self.iron = torch.as_tensor(np.flatnonzero(self.tags == synth.IRON).astype(np.int32), device=dev)
+        self.iron_rows = torch.arange(self.iron.numel(), dtype=torch.int32, device=dev)
         sigma = np.where(self.tags == synth.IRON, cfg.sigma_iron, 0.0)
         self.has_sigma = bool(np.any(sigma != 0.0))
         self.m_sigma = self.plan.mass(torch.as_tensor(sigma, dtype=torch.float64, device=dev)) \
@@ -245,8 +250,8 @@ class TransientProblem:
         bscale = None
         if seed_nu is not None:
             bscale = torch.empty(self.plan.num_elements, dtype=torch.float64, device="cuda")
-            _lib.check(self.lib.mag_seed_midpoint(self.plan._h, _ptr(x), _ptr(seed_nu), _ptr(bscale),
-                                                  _lib.stream_ptr()))
+            _lib.check(self.lib.mag_seed_midpoint(self.plan._h, _ptr(x), _ptr(seed_nu), cfg.seed_max_scale,
+                                                  _ptr(bscale), _lib.stream_ptr()))
         for it_n in range(1, cfg.max_newton + 1):
             e0 = tm.start()
             vals, r = self.residual(x, x_prev, F, True, bscale if it_n == 1 else None)
@@ -371,7 +376,9 @@ def run(prob: TransientProblem, first: int, last: int, x_prev, b_hist, mode: str
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
             seed = torch.zeros(prob.plan.num_elements, dtype=torch.float64, device="cuda")
-            predictor.predict_nu(features(prob, b1, b2, t), prob.iron, seed, nu_min=1.0, nu_max=NU0)
+            ratio = torch.empty(prob.iron.numel(), dtype=torch.float64, device="cuda")
+            predictor.predict_nu(features(prob, b1, b2, t), prob.iron_rows, ratio, nu_min=1e-3, nu_max=1e3)
+            seed[ir] = prob.element_nu(x)[ir] * ratio
             e1.record()
             e1.synchronize()
             mlp_ms = e0.elapsed_time(e1)
@@ -398,16 +405,22 @@ def run(prob: TransientProblem, first: int, last: int, x_prev, b_hist, mode: str
 
 
 def training_set(prob: TransientProblem, rec: RunRecord, first: int, last: int):
-    """(features, nu) pairs of steps first..last from a plain run recorded from step 1."""
+    """(features, nu_t / nu_{t-1}) pairs of steps first..last from a plain run recorded from step 1.
+
+    The network learns the step's change of reluctivity; the seed multiplies it onto the
+    reluctivity evaluated exactly at x_{t-1}, so its error scales with the change, not with nu.
+    """
     cfg = prob.cfg
     n = prob.iron.numel()
     zero = torch.zeros(n, dtype=torch.float32, device="cuda")
+    nu0 = prob.element_nu(torch.zeros(prob.num_dofs, dtype=torch.float64, device="cuda"))[prob.iron.long()]
     fs, ys = [], []
     for s in range(first, last + 1):
         b1 = rec.bmag[s - 2] if s >= 2 else zero
         b2 = rec.bmag[s - 3] if s >= 3 else zero
         fs.append(features(prob, b1, b2, s * cfg.dt))
-        ys.append(rec.nu[s - 1].double())
+        prev = rec.nu[s - 2].double() if s >= 2 else nu0
+        ys.append(rec.nu[s - 1].double() / prev)
     return torch.cat(fs), torch.cat(ys)
 
 

@@ -168,7 +168,7 @@ def test_seeded_jacobian_with_unit_scale_is_the_jacobian():
     nu = torch.empty(plan.num_elements, dtype=torch.float64, device="cuda")
     _lib.check(L.mag_element_nu(plan._h, _ptr(x), _ptr(nu), None, _lib.stream_ptr()))
     beta = torch.empty_like(nu)
-    _lib.check(L.mag_seed_midpoint(plan._h, _ptr(x), _ptr(nu), _ptr(beta), _lib.stream_ptr()))
+    _lib.check(L.mag_seed_midpoint(plan._h, _ptr(x), _ptr(nu), 4.0, _ptr(beta), _lib.stream_ptr()))
     from magpackage_b200.material import NU0
 
     iron = torch.as_tensor(tags == synth.IRON, device="cuda")
@@ -179,20 +179,20 @@ def test_seeded_jacobian_with_unit_scale_is_the_jacobian():
     assert torch.all(beta[~iron] == 1.0)
 
 
-def test_learned_warm_start_against_plain():
-    """Plain warm start on every step; an MLP trained on the first half seeds the second half's
-    first Jacobian. Every step of every mode reaches the same RHS-relative tolerance; seeding
-    with the converged nu (the bound for any predictor) saves Newton iterations; the network's
-    nu is close to the converged one, and its seed costs at most a bounded number of extra
-    iterations (at these small steps the plain warm start is already within 3-5 iterations)."""
+def test_learned_warm_start_beats_plain():
+    """The config-4 time discretisation (dt = 1e-4, 200 steps) on a 20 x 20 x 10 box: plain warm
+    start on every step; an MLP trained on steps 1-100 seeds the first Jacobian of steps
+    101-200. Every step of every mode reaches the same RHS-relative tolerance; the learned
+    seed needs fewer Newton iterations and fewer assemblies than the plain warm start, and
+    seeding with the converged nu (the bound for any predictor) does better still."""
     from magpackage_b200.transient import TransientConfig, compare
 
-    cfg = TransientConfig(nx=20, ny=20, nz=10, steps=40, dt=5e-4)
-    out = compare(cfg, epochs=120)
+    out = compare(TransientConfig(nx=20, ny=20, nz=10), epochs=120)
     p, l, i = out["plain"], out["learned"], out["ideal"]
     assert p["converged"] and l["converged"] and i["converged"]
     assert max(p["max_res_over_tol"], l["max_res_over_tol"], i["max_res_over_tol"]) <= 1.0
-    assert out["train"]["loss_last"] < 0.1 * out["train"]["loss_first"]
-    assert i["newton"] < p["newton"]
-    assert l["nu_rel_err_median"] < 0.2
-    assert l["newton"] <= 1.25 * p["newton"]
+    print({k: (out[k]["newton"], out[k]["assemblies"], round(out[k]["gpu_ms"])) for k in ("plain", "learned", "ideal")})
+    assert out["train"]["loss_last"] < 0.5 * out["train"]["loss_first"]
+    assert l["newton"] < p["newton"] and l["assemblies"] < p["assemblies"]
+    assert i["newton"] <= l["newton"]
+    assert l["nu_rel_err_median"] < 0.05
