@@ -48,3 +48,14 @@ def test_version_and_error_text_without_gpu():
     # argument validation happens before any CUDA call
     rc = lib.mag_mesh_get_info(None, None)
     assert rc == -1 and b"bad arguments" in lib.mag_last_error()
+
+
+def test_mex_entry_points_accept_an_empty_mesh():
+    """The reference gateways return empty triplets for zero elements; so do these, without
+    touching the GPU (so this runs on the CPU)."""
+    L = _lib.load()
+    p = (ctypes.c_double * 4)()
+    args_j = [p, 1, p, 0, p, p, p, p, 1, p, 4, p, p, p, p, 1, p, 1, p, 4, p, p, p, 1, p, p, p, p, p]
+    assert L.mag_mex_jacobian(*args_j) == 0
+    assert L.mag_mex_curl_curl(p, 1, p, 0, p, p, p, p, 4, p, p, p, p) == 0
+    assert L.mag_mex_mass(p, 1, p, 0, p, p, None, 0, p, 4, p, p, p, p) == 0

@@ -424,3 +424,46 @@ def test_batched_complex_matches_oracle(oracle_port):
             im = host(v.imag.contiguous())
             assert bits_equal(im, omega * mref[2])
     batch.close()
+
+
+# ---- wide rows ---------------------------------------------------------------------------
+
+def _pinwheel(n_blades=12, seed=0):
+    """n tetrahedra around one edge (nodes 0, 1 on the axis, a ring of n nodes): that edge's
+    CSR row has 3n + 1 entries, more than the compact 31-slot position format holds."""
+    rng = np.random.default_rng(seed)
+    ang = 2 * np.pi * np.arange(n_blades) / n_blades
+    ring = np.stack([np.cos(ang), np.sin(ang), 0.5 + 0.05 * rng.normal(size=n_blades)], axis=1)
+    P = np.vstack([[0.0, 0.0, 0.0], [0.0, 0.0, 1.0], ring])
+    T = np.array([[0, 1, 2 + i, 2 + (i + 1) % n_blades] for i in range(n_blades)], dtype=np.int32)
+    # orient every tetrahedron positively
+    for e in range(T.shape[0]):
+        a, b, c, d = P[T[e]]
+        if np.dot(np.cross(b - a, c - a), d - a) < 0:
+            T[e, [2, 3]] = T[e, [3, 2]]
+    return P, T
+
+
+def test_wide_rows_match_oracle_on_every_schedule(oracle_port):
+    P, T = _pinwheel()
+    tags = np.where(np.arange(T.shape[0]) % 2 == 0, synth.IRON, synth.AIR).astype(np.int32)
+    edges, t2e, sign, m = make_case(oracle_port, P, T, tags)
+    E = edges.shape[0]
+    pk = material.pack_material_data(synth.standard_materials())
+    sol = np.random.default_rng(7).normal(0, 0.5, E)
+    qw, val, curl = quadrature.reference_data(2)
+    I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, qw, curl, pk, True)
+    ref = oracle_matrix(oracle_port, I, J, V, E, False)
+    plan = AssemblyPlan(P, T, t2e, E, tags, sign)
+    assert plan.info.wide_positions == 1 and plan.info.max_row_nnz > 31
+    plan.set_materials(pk)
+    x = dev(sol)
+    for sch in SCHEDULES:
+        plan.set_schedule(sch)
+        v, r = plan.jacobian(x)
+        plan.check()
+        assert_csr_equal(plan.row_ptr, plan.col_idx, v, ref)
+        assert bits_equal(host(r), oracle_port.sparse_vec(Ri, Rv, E)), sch
+    K = plan.stiffness(dev(np.full(T.shape[0], 800.0)))
+    Ik, Jk, Vk = oracle_port.curl_curl(m, np.full(T.shape[0], 800.0), qw, curl)
+    assert_csr_equal(plan.row_ptr, plan.col_idx, K, oracle_matrix(oracle_port, Ik, Jk, Vk, E, False))
