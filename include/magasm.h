@@ -212,6 +212,9 @@ int mag_batch_assemble(mag_batch *batch, void *stream);
  * during creation (times[] must hold mag_batch_variants() entries). */
 int mag_batch_variants(void);
 int mag_batch_tuning(const mag_batch *batch, int *chosen, double *times_ms, char *name, int name_len);
+/* Use variant `variant` (0 .. mag_batch_variants()-1) instead of the tuned one and
+ * capture it again; MAG_E_UNSUPPORTED if it is not available for these meshes. */
+int mag_batch_select(mag_batch *batch, int variant);
 int mag_batch_destroy(mag_batch *batch);
 
 /* ---- per-element reluctivity predictor (no counterpart in the reference) ---- */

@@ -70,6 +70,7 @@ _PROTOS = {
     "mag_batch_assemble": ([_vp, _vp], _int),
     "mag_batch_variants": ([], _int),
     "mag_batch_tuning": ([_vp, C.POINTER(_int), _dp, C.c_char_p, _int], _int),
+    "mag_batch_select": ([_vp, _int], _int),
     "mag_batch_destroy": ([_vp], _int),
     "mag_mlp_num_params": ([], _int),
     "mag_mlp_create": ([C.POINTER(C.c_float), C.POINTER(_vp)], _int),

@@ -243,6 +243,7 @@ int batch_launch(const BatchState &b, int variant, cudaStream_t s) {
 }
 
 int batch_num_variants() { return kNumVariants; }
+bool batch_variant_available(const BatchState &b, int v) { return v >= 0 && v < kNumVariants && b.var[v].nitems > 0; }
 const char *batch_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : ""; }
 int batch_variant_threads(int v) { return kVariants[v].threads; }
 

@@ -43,6 +43,7 @@ struct BatchState {
 int batch_build(BatchState *b, cudaStream_t s);
 int batch_launch(const BatchState &b, int variant, cudaStream_t s);
 int batch_num_variants();
+bool batch_variant_available(const BatchState &b, int v);
 const char *batch_variant_name(int v);
 int batch_variant_threads(int v);
 void batch_free_variants(BatchState *b);

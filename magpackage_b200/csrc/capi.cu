@@ -779,6 +779,35 @@ extern "C" {
 
 int mag_batch_variants(void) { return batch_num_variants(); }
 
+}  // extern "C"
+
+namespace {
+// Capture the chosen variant's launch in a CUDA graph (replacing any earlier one); capture
+// needs a stream other than the legacy default.
+int capture_batch(mag_batch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return MAG_E_CUDA;
+    cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+        batch_launch(b->st, b->chosen, cs);
+        ce = cudaStreamEndCapture(cs, &b->graph);
+    }
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    cudaStreamDestroy(cs);
+    if (ce != cudaSuccess) {
+        set_error("batch graph capture failed: %s", cudaGetErrorString(ce));
+        return MAG_E_CUDA;
+    }
+    return MAG_OK;
+}
+}  // namespace
+
+extern "C" {
+
 int mag_batch_create(mag_mesh *const *meshes, int n, const double *const *d_nu, const double *const *d_sigma,
                      const double *omega, double *const *d_vals, mag_batch **out, void *stream) {
     if (!meshes || n < 1 || !d_nu || !omega || !d_vals || !out) {
@@ -829,6 +858,8 @@ int mag_batch_create(mag_mesh *const *meshes, int n, const double *const *d_nu, 
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return fail(MAG_E_CUDA);
     double best = 1e300;
     for (int v = 0; v < batch_num_variants(); v++) {
+        b->times[v] = -1.0;  // not available for these meshes
+        if (!batch_variant_available(b->st, v)) continue;
         rc = batch_launch(b->st, v, s);  // warm-up
         if (rc != MAG_OK) break;
         cudaEventRecord(e0, s);
@@ -849,22 +880,23 @@ int mag_batch_create(mag_mesh *const *meshes, int n, const double *const *d_nu, 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != MAG_OK) return fail(rc);
-    // capture the chosen launch (capture needs a stream other than the legacy default)
-    cudaStream_t cs;
-    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return fail(MAG_E_CUDA);
-    cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-    if (ce == cudaSuccess) {
-        batch_launch(b->st, b->chosen, cs);
-        ce = cudaStreamEndCapture(cs, &b->graph);
-    }
-    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&b->exec, b->graph, 0);
-    cudaStreamDestroy(cs);
-    if (ce != cudaSuccess) {
-        set_error("mag_batch_create: graph capture failed: %s", cudaGetErrorString(ce));
-        return fail(MAG_E_CUDA);
-    }
+    rc = capture_batch(b);
+    if (rc != MAG_OK) return fail(rc);
     *out = b;
     return MAG_OK;
+}
+
+int mag_batch_select(mag_batch *b, int variant) {
+    if (!b || variant < 0 || variant >= batch_num_variants()) {
+        set_error("mag_batch_select: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (!batch_variant_available(b->st, variant)) {
+        set_error("mag_batch_select: variant %d is not available for these meshes", variant);
+        return MAG_E_UNSUPPORTED;
+    }
+    b->chosen = variant;
+    return capture_batch(b);
 }
 
 int mag_batch_assemble(mag_batch *b, void *stream) {

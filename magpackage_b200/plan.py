@@ -214,6 +214,10 @@ class ComplexBatch:
         _lib.check(self._lib.mag_batch_assemble(self._h, _lib.stream_ptr(stream)))
         return self.values
 
+    def select(self, variant: int):
+        """Replay `variant` from now on instead of the tuned one."""
+        _lib.check(self._lib.mag_batch_select(self._h, int(variant)))
+
     def tuning(self):
         nv = self._lib.mag_batch_variants()
         chosen = C.c_int()

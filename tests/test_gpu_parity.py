@@ -416,13 +416,16 @@ def test_batched_complex_matches_oracle(oracle_port):
     batch = ComplexBatch(plans, nus, sigmas, [c[4] for c in cases])
     chosen, times, name = batch.tuning()
     assert 0 <= chosen < len(times) and times[chosen] == times[times > 0].min() and name
-    for rep in range(2):  # graph replay is repeatable
-        vals = batch.assemble()
-        torch.cuda.synchronize()
-        for plan, v, (kref, mref, omega) in zip(plans, vals, refs):
-            assert_csr_equal(plan.row_ptr, plan.col_idx, v.real.contiguous(), kref)
-            im = host(v.imag.contiguous())
-            assert bits_equal(im, omega * mref[2])
+    assert np.all(times > 0)  # every variant, shared-element ones included, ran on these meshes
+    for variant in [chosen] + [v for v in range(len(times)) if v != chosen]:
+        batch.select(variant)
+        for rep in range(2):  # graph replay is repeatable
+            vals = batch.assemble()
+            torch.cuda.synchronize()
+            for plan, v, (kref, mref, omega) in zip(plans, vals, refs):
+                assert_csr_equal(plan.row_ptr, plan.col_idx, v.real.contiguous(), kref)
+                im = host(v.imag.contiguous())
+                assert bits_equal(im, omega * mref[2]), variant
     batch.close()
 
 
