@@ -134,6 +134,41 @@ __device__ __forceinline__ void tmem_row(uint32_t tmem, float out[kH]) {
     for (int i = 0; i < kH; i++) out[i] = __uint_as_float(r[i]);
 }
 
+// Columns c..c+15 of this thread's accumulator row from TMEM.
+__device__ __forceinline__ void tmem_cols16(uint32_t tmem, int c, float out[16]) {
+    const uint32_t lane_base = (uint32_t)((threadIdx.x >> 5) * 32) << 16;
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(tmem + lane_base + (uint32_t)c));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) out[i] = __uint_as_float(r[i]);
+}
+
+// A hidden layer's epilogue, 16 columns at a time (few live registers): z = acc + b,
+// h = SiLU(z) as BF16 into the next layer's input image; z kept for training.
+__device__ __forceinline__ void hidden_epilogue(uint32_t tmem, const float *bias, __nv_bfloat16 *img, int row_t,
+                                                float *z_row) {
+#pragma unroll
+    for (int c = 0; c < kH; c += 16) {
+        float z[16];
+        tmem_cols16(tmem, c, z);
+        __align__(16) __nv_bfloat162 hp[8];
+#pragma unroll
+        for (int i = 0; i < 16; i++) z[i] += bias[c + i];
+#pragma unroll
+        for (int i = 0; i < 8; i++) hp[i] = __floats2bfloat162_rn(silu(z[2 * i]), silu(z[2 * i + 1]));
+        *reinterpret_cast<uint4 *>(img + core_off(row_t, c, kH)) = *reinterpret_cast<uint4 *>(hp);
+        *reinterpret_cast<uint4 *>(img + core_off(row_t, c + 8, kH)) = *reinterpret_cast<uint4 *>(hp + 4);
+        if (z_row)
+#pragma unroll
+            for (int i = 0; i < 16; i++) z_row[c + i] = z[i];
+    }
+}
+
 // Write this thread's row of 64 values as BF16 into a K=64 core-matrix image.
 __device__ __forceinline__ void put_row64(__nv_bfloat16 *img, int row, const float v[kH]) {
 #pragma unroll
@@ -198,7 +233,7 @@ __device__ __forceinline__ bool run_layer(Smem &S, const __nv_bfloat16 *W, int K
 
 // ---- forward ---------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kRows, 1) k_mlp_forward(MlpForwardArgs a) {
+__global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     Smem &S = *reinterpret_cast<Smem *>(smem_raw);
     const int t = threadIdx.x;
@@ -238,45 +273,32 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp_forward(MlpForwardArgs a) {
             *reinterpret_cast<uint4 *>(S.act + core_off(t, 0, 16)) = *reinterpret_cast<uint4 *>(v);
             *reinterpret_cast<uint4 *>(S.act + core_off(t, 8, 16)) = *reinterpret_cast<uint4 *>(v + 8);
         }
-        float z[kH], h[kH];
+        float *zr = (a.z_out && valid) ? a.z_out + row * 3 * kH : nullptr;
         // layer 1
+        // (a completed MMA has read its input image; the next layer's issue barrier orders
+        // this thread's TMEM reads and image writes before the next MMA)
         if (!run_layer(S, W1, 16, phase)) break;
-        tmem_row(S.tmem, z);
-#pragma unroll
-        for (int o = 0; o < kH; o++) {
-            z[o] += sb1[o];
-            h[o] = silu(z[o]);
-        }
-        if (a.z_out && valid)
-            for (int o = 0; o < kH; o++) a.z_out[(row * 3 + 0) * kH + o] = z[o];
-        tc_fence_before();
-        __syncthreads();  // every thread has read TMEM before the next MMA writes it
-        put_row64(S.act, t, h);
+        hidden_epilogue(S.tmem, sb1, S.act, t, zr);
         // layer 2
         if (!run_layer(S, W2, kH, phase)) break;
-        tmem_row(S.tmem, z);
-#pragma unroll
-        for (int o = 0; o < kH; o++) {
-            z[o] += sb2[o];
-            h[o] = silu(z[o]);
-        }
-        if (a.z_out && valid)
-            for (int o = 0; o < kH; o++) a.z_out[(row * 3 + 1) * kH + o] = z[o];
-        tc_fence_before();
-        __syncthreads();
-        put_row64(S.act, t, h);
-        // layer 3
+        hidden_epilogue(S.tmem, sb2, S.act, t, zr ? zr + kH : nullptr);
+        // layer 3 and the 64 -> 1 output, 16 columns at a time
         if (!run_layer(S, W3, kH, phase)) break;
-        tmem_row(S.tmem, z);
         float y = 0.0f;
 #pragma unroll
-        for (int o = 0; o < kH; o++) {
-            z[o] += sb3[o];
-            y += sw4[o] * silu(z[o]);
+        for (int c = 0; c < kH; c += 16) {
+            float z[16];
+            tmem_cols16(S.tmem, c, z);
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                z[i] += sb3[c + i];
+                y += sw4[c + i] * silu(z[i]);
+            }
+            if (zr)
+#pragma unroll
+                for (int i = 0; i < 16; i++) zr[2 * kH + c + i] = z[i];
         }
         y += S.vec[4 * kH];
-        if (a.z_out && valid)
-            for (int o = 0; o < kH; o++) a.z_out[(row * 3 + 2) * kH + o] = z[o];
         if (valid) {
             if (a.y_out) a.y_out[row] = y;
             if (a.nu_out) {  // nu = exp(y * scale + shift), clamped to [nu_min, nu_max]
