@@ -178,6 +178,14 @@ int mag_assemble_mass(mag_mesh *mesh, const double *d_sigma, double *d_vals, voi
  * d_js [Ne][3] current density per element; d_out [num_dofs]. */
 int mag_assemble_source(mag_mesh *mesh, const double *d_js, double *d_out, void *stream);
 
+/* Winding (coil current) vector C = sparse(I(valid), 1, V(valid), num_dofs, 1) as a dense
+ * d_out [num_dofs] (assemble_winding_kernel_mex.cpp:13-127 + Assembler.m:134-161): the
+ * elements tagged coil_id, direction d_dir_field [Ne][3] (device; NULL = the uniform host
+ * direction dir[3]) times scale (Turns / CrossSectionArea), integrated against the basis
+ * of mag_mesh_set_quadrature's ValRef. Summed in ascending element order. */
+int mag_assemble_winding(mag_mesh *mesh, int coil_id, const double *d_dir_field, const double *dir,
+                         double scale, double *d_out, void *stream);
+
 /* Element magnetic flux density B [Ne][3] and |B|^2 [Ne] at the solution
  * d_sol (the per-element curl of PostProcessor.computeElementB,
  * src/post/PostProcessor.m:64-126, evaluated as the Jacobian kernel does). */
@@ -320,6 +328,56 @@ int mag_mex_curl_curl(const double *P, int64_t Nn, const double *T, int64_t Ne, 
 int mag_mex_mass(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
                  const double *Signs, const double *Coeffs, int64_t ncoeffs, const double *Qw,
                  int nq, const double *ValRef, double *I, double *J, double *V);
+
+/* [I,V] = assemble_source_kernel_mex(P,T,Dofs,Signs,Js,Qw,ValRef)
+ * (src/mex/assemble_source_kernel_mex.cpp:16-114): Js [3 x Ne]; outputs 6*Ne. */
+int mag_mex_source(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                   const double *Signs, const double *Js, const double *Qw, int nq, const double *ValRef,
+                   double *I, double *V);
+
+/* [I,V] = assemble_winding_kernel_mex(P,T,Dofs,Signs,Tags,CoilID,DirField,UniDir,Scale,Qw,ValRef)
+ * (src/mex/assemble_winding_kernel_mex.cpp:13-127): DirField [3 x Ne] or NULL (the
+ * empty []: UniDir [3] for every element); I = V = 0 for elements outside the coil.
+ * Outputs 6*Ne. */
+int mag_mex_winding(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                    const double *Signs, const double *Tags, double CoilID, const double *DirField,
+                    const double *UniDir, double Scale, const double *Qw, int nq, const double *ValRef,
+                    double *I, double *V);
+
+/* ---- MATLAB sparse results of the MEX-compatible entry points --------------
+ * The sparse() that Assembler.m applies to the gateways' triplets
+ * (Assembler.m:37-38 stiffness, :52-53 and :71-72 mass, :205-215 Jacobian and
+ * residual) done on the GPU: the host receives MATLAB's compressed-column
+ * storage (jc [n+1], ir [nnz] as 64-bit mwIndex, pr [nnz]) instead of 36*Ne
+ * triplets. Duplicates are summed in ascending element order, exact zeros are
+ * dropped and entries of missing dofs (Dofs == 0) are skipped, as the
+ * (I > 0) & (J > 0) filter and sparse() do. The MEX gateways return it when
+ * given their optional trailing argument. */
+typedef struct mag_sparse mag_sparse;
+
+/* J = sparse(I, J, V, Ndof, Ndof) and R = full(sparse(R_idx, 1, R_val, Ndof, 1))
+ * of mag_mex_jacobian's outputs (same inputs). R is a host buffer [Ndof].
+ * *J_out is left NULL when calc_j == 0. */
+int mag_mex_jacobian_sparse(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                            const double *Signs, const double *Tags, const double *SolA, int64_t Ndof,
+                            const double *Qw, int nq, const double *CurlRef, const double *lin,
+                            const double *isNon, const double *maxB, int nmat, const double *brk, int nbrk,
+                            const double *coe, int ncoe, const double *start, const double *cnt,
+                            const double *coeStart, int calc_j, mag_sparse **J_out, double *R);
+/* K = sparse(I, J, V, Ndof, Ndof) of mag_mex_curl_curl's outputs. */
+int mag_mex_curl_curl_sparse(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                             const double *Signs, const double *Nu, const double *Qw, int nq,
+                             const double *CurlRef, int64_t Ndof, mag_sparse **out);
+/* M = sparse(I, J, V, Ndof, Ndof) of mag_mex_mass's outputs. */
+int mag_mex_mass_sparse(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                        const double *Signs, const double *Coeffs, int64_t ncoeffs, const double *Qw, int nq,
+                        const double *ValRef, int64_t Ndof, mag_sparse **out);
+/* Size (n x n) and number of stored entries. */
+int mag_sparse_info(const mag_sparse *sp, int64_t *n, int64_t *nnz);
+/* Copy into host arrays jc [n+1], ir [nnz], pr [nnz] (mxGetJc / mxGetIr / mxGetPr
+ * of mxCreateSparse(n, n, nnz, mxREAL)). */
+int mag_sparse_copy(const mag_sparse *sp, uint64_t *jc, uint64_t *ir, double *pr);
+int mag_sparse_destroy(mag_sparse *sp);
 
 /* Allocation-free form of mag_mex_jacobian, for callers that cannot allocate
  * device memory: a MEX function working on mxGPUArray buffers owned by

@@ -54,6 +54,7 @@ _PROTOS = {
     "mag_assemble_stiffness": ([_vp, _vp, _vp, _vp], _int),
     "mag_assemble_mass": ([_vp, _vp, _vp, _vp], _int),
     "mag_assemble_source": ([_vp, _vp, _vp, _vp], _int),
+    "mag_assemble_winding": ([_vp, _int, _vp, _dp, C.c_double, _vp, _vp], _int),
     "mag_element_b": ([_vp, _vp, _vp, _vp, _vp], _int),
     "mag_element_nu": ([_vp, _vp, _vp, _vp, _vp], _int),
     "mag_assemble_hbfem": ([_vp, _vp, _vp, _int, _vp, _vp, _vp, _vp, _int, _vp, _vp, _vp, _vp], _int),
@@ -89,6 +90,19 @@ _PROTOS = {
                           _dp], _int),
     "mag_mex_curl_curl": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _int, _dp, _dp, _dp, _dp], _int),
     "mag_mex_mass": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _i64, _dp, _int, _dp, _dp, _dp, _dp], _int),
+    "mag_mex_source": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _int, _dp, _dp, _dp], _int),
+    "mag_mex_winding": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, C.c_double, _dp, _dp, C.c_double, _dp, _int,
+                         _dp, _dp, _dp], _int),
+    "mag_mex_jacobian_sparse": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _i64, _dp, _int, _dp, _dp, _dp,
+                                 _dp, _int, _dp, _int, _dp, _int, _dp, _dp, _dp, _int, C.POINTER(_vp), _dp],
+                                _int),
+    "mag_mex_curl_curl_sparse": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _int, _dp, _i64, C.POINTER(_vp)],
+                                 _int),
+    "mag_mex_mass_sparse": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _i64, _dp, _int, _dp, _i64, C.POINTER(_vp)],
+                            _int),
+    "mag_sparse_info": ([_vp, C.POINTER(_i64), C.POINTER(_i64)], _int),
+    "mag_sparse_copy": ([_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _dp], _int),
+    "mag_sparse_destroy": ([_vp], _int),
     "mag_mex_jacobian_noalloc": ([_vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _dp, _int, _dp, _dp,
                                   _dp, _dp, _int, _dp, _int, _dp, _int, _dp, _dp, _dp, _int, _vp, _vp,
                                   _vp, _vp, _vp, _vp], _int),

@@ -10,9 +10,12 @@ names (snake_case), argument meaning and error behaviour:
                     numbered in edge order; ``pack_for_kernel`` (:124-130).
 * ``Assembler``  -- src/Assembler.m: ``assemble_stiffness`` (:26-39),
                     ``assemble_mass`` (:41-57), ``assemble_mass_weighted``
-                    (:59-76), ``assemble_source`` (:78-97), ``assemble_jacobian``
-                    (:182-231), ``expand_material_map`` (:240-268) and
-                    ``pack_material_data`` (:270-304).
+                    (:59-76), ``assemble_source`` (:78-97), ``assemble_winding``
+                    (:134-180), ``assemble_jacobian`` (:182-231),
+                    ``expand_material_map`` (:240-268) and ``pack_material_data``
+                    (:270-304).
+* ``Winding``    -- src/Winding.m (coil region, turns, cross-section, unit
+                    direction or a per-element direction field).
 
 Indices are 0-based here (the reference's are 1-based). Matrices come back as
 ``CSR`` objects holding CUDA tensors. With ``matlab_storage=True`` (default)
@@ -51,6 +54,31 @@ class CSR:
         A = torch.sparse_csr_tensor(self.row_ptr, self.col_idx.to(torch.int64), self.values,
                                     size=self.shape)
         return A @ x
+
+
+@dataclass
+class Winding:
+    """src/Winding.m: a coil on region RegionID. ``create`` normalises the direction
+    as the constructor does (Winding.m:18-31); DirectionField [Ne, 3], when set, takes
+    precedence over Direction in the assembly."""
+
+    Name: str
+    RegionID: int
+    Turns: float
+    Resistance: float
+    CrossSectionArea: float
+    Direction: np.ndarray
+    DirectionField: np.ndarray | None = None
+
+    @classmethod
+    def create(cls, name, region_id, turns, resistance, area, direction):
+        d = np.asarray(direction, dtype=np.float64).ravel()[:3]
+        n = float(np.linalg.norm(d))
+        return cls(name, int(region_id), float(turns), float(resistance), float(area),
+                   d / n if n > 0 else np.zeros(3))
+
+    def set_direction_field(self, field):
+        self.DirectionField = None if field is None else np.asarray(field, dtype=np.float64)
 
 
 class Mesh:
@@ -193,6 +221,20 @@ class Assembler:
             else:
                 raise ValueError("Source must be [3x1] or [Ne x 3].")
         return self.plan.source(self._dev(js))
+
+    def assemble_winding(self, winding) -> torch.Tensor:
+        """Coil vector C [num_dofs] of one Winding (Turns / CrossSectionArea times its
+        direction, Assembler.m:157-166), or [num_dofs, k] for a list (:175-178)."""
+        if isinstance(winding, (list, tuple)):
+            return torch.stack([self.assemble_winding(w) for w in winding], dim=1)
+        scale = winding.Turns / winding.CrossSectionArea
+        field = None
+        if winding.DirectionField is not None and np.size(winding.DirectionField):
+            f = np.asarray(winding.DirectionField, dtype=np.float64)
+            if f.shape != (self.Mesh.num_elements, 3):
+                raise ValueError("DirectionField must be [Ne x 3]")
+            field = self._dev(f)
+        return self.plan.winding(winding.RegionID, winding.Direction, scale, dir_field=field)
 
     def assemble_jacobian(self, solution_a, matlib, calc_j: bool = True):
         p = self.plan

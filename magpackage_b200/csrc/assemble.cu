@@ -303,6 +303,62 @@ __global__ void __launch_bounds__(128) k_source_elems(ElemData m, const double *
     for (int i = 0; i < 6; i++) dst[i * kScratchStride + 6] = flip(f[i], (sb >> i) & 1);
 }
 
+// ---- winding (coil current) vector ---------------------------------------------
+// assemble_winding_kernel_mex.cpp:13-127 per element: zero outside the coil region
+// (:54-61), else the direction (per-element field or uniform, :78-87) times the scale
+// (:90-92), mapped by J^{-1} (:96) and integrated against the reference basis with
+// no cut-off (:99-114), signed (:124). Writes the residual slot of the element scratch
+// and/or the reference's (I, V) pairs (I = 0 outside the coil).
+struct WindingArgs {
+    int coil;
+    const double *field;  // [Ne][3] or NULL
+    double dir[3];
+    double scale;
+};
+
+__global__ void __launch_bounds__(128) k_winding_elems(ElemData m, WindingArgs wa, QuadParams qp,
+                                                       double *__restrict__ scratch, double *__restrict__ I,
+                                                       double *__restrict__ V) {
+    __shared__ double sref[18 * kMaxQuad];
+    for (int i = threadIdx.x; i < 18 * qp.nq; i += blockDim.x) sref[i] = qp.val_ref[i];
+    __syncthreads();
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    const bool in_coil = (int)m.tags[e] == wa.coil;
+    unsigned sb = 0;
+    if (in_coil) {
+        const int4 t = m.tet[e];
+        sb = m.signbits ? m.signbits[e] : derived_signs(t);
+        Geo g;
+        geometry(m.xyz, t, g);
+        double iv[3][3];
+        inverse3(g, iv);
+        const double *d = wa.field ? wa.field + 3 * e : wa.dir;
+        const double jp[3] = {d[0] * wa.scale, d[1] * wa.scale, d[2] * wa.scale};
+        double jr[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) jr[r] = iv[r][0] * jp[0] + iv[r][1] * jp[1] + iv[r][2] * jp[2];
+        for (int q = 0; q < qp.nq; q++) {
+            const double w = qp.qw[q] * g.adet;
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                const double r[3] = {sref[i + 18 * q], sref[i + 6 + 18 * q], sref[i + 12 + 18 * q]};
+                f[i] = f[i] + dot3(jr, r) * w;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        const double v = in_coil ? flip(f[i], (sb >> i) & 1) : 0.0;
+        if (scratch) scratch[e * kScratchPerElem + i * kScratchStride + 6] = v;
+        if (I) {
+            I[6 * e + i] = in_coil ? (double)(m.dofs[6 * e + i] + 1) : 0.0;
+            V[6 * e + i] = v;
+        }
+    }
+}
+
 // ---- element B (post-processing / predictor features) -------------------------
 
 __global__ void __launch_bounds__(128) k_element_b(ElemData m, const double *__restrict__ sol,
@@ -469,6 +525,13 @@ int launch_mass_elems(const ElemData &m, const double *sigma, const QuadParams &
 int launch_source_elems(const ElemData &m, const double *js, const QuadParams &qp, double *scratch,
                         cudaStream_t s) {
     k_source_elems<<<blocks(m.ne, 128), 128, 0, s>>>(m, js, qp, scratch);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+int launch_winding_elems(const ElemData &m, int coil, const double *field, const double dir[3], double scale,
+                         const QuadParams &qp, double *scratch, double *I, double *V, cudaStream_t s) {
+    WindingArgs wa{coil, field, {dir[0], dir[1], dir[2]}, scale};
+    k_winding_elems<<<blocks(m.ne, 128), 128, 0, s>>>(m, wa, qp, scratch, I, V);
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
 

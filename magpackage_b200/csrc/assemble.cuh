@@ -19,6 +19,10 @@ int launch_mass_elems(const ElemData &m, const double *sigma, const QuadParams &
                       cudaStream_t s);
 int launch_source_elems(const ElemData &m, const double *js, const QuadParams &qp, double *scratch,
                         cudaStream_t s);
+// Winding vector (coil region `coil`, direction field [Ne][3] or uniform dir, times scale):
+// residual slot of `scratch` and/or the reference's (I, V) pairs (either may be NULL).
+int launch_winding_elems(const ElemData &m, int coil, const double *field, const double dir[3], double scale,
+                         const QuadParams &qp, double *scratch, double *I, double *V, cudaStream_t s);
 int launch_element_b(const ElemData &m, const double *sol, double *b, double *bsq, cudaStream_t s,
                      const MaterialParams *mp = nullptr, double *nu = nullptr, double *dnu = nullptr);
 int launch_rows_reduce(const RowPlan &rp, int max_row, const double *scratch, double *vals,

@@ -668,6 +668,21 @@ int mag_assemble_source(mag_mesh *m, const double *d_js, double *d_out, void *st
     return finish(s);
 }
 
+int mag_assemble_winding(mag_mesh *m, int coil_id, const double *d_dir_field, const double *dir, double scale,
+                         double *d_out, void *stream) {
+    MAG_TRY(require_ready(m, false));
+    if (!d_out || (!d_dir_field && !dir)) {
+        set_error("mag_assemble_winding: bad arguments");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const double zero[3] = {0.0, 0.0, 0.0};
+    MAG_TRY(launch_winding_elems(m->elems(), coil_id, d_dir_field, dir ? dir : zero, scale, m->qp, m->scratch,
+                                 nullptr, nullptr, s));
+    MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, nullptr, d_out, s));
+    return finish(s);
+}
+
 int mag_element_b(mag_mesh *m, const double *d_sol, double *d_b, double *d_bsq, void *stream) {
     MAG_TRY(require_ready(m, false));
     if (!d_sol || (!d_b && !d_bsq)) {
@@ -1226,6 +1241,40 @@ int mex_download(MexMesh &mm, int64_t Ne, int calcj, double *I, double *J, doubl
     return MAG_OK;
 }
 
+// The Jacobian element phase of the MEX entry points: upload, materials, quadrature,
+// element blocks and residual entries into mm.scratch.
+struct MexJacobian {
+    MexMesh mm;
+    MaterialStore ms{};
+    double *q = nullptr;
+    Dev sol;
+    explicit MexJacobian(cudaStream_t s) : mm(s), sol(s) {}
+    ~MexJacobian() {
+        if (ms.mem) cudaFree(ms.mem);
+        if (q) cudaFree(q);
+    }
+    int run(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs, const double *Signs,
+            const double *Tags, const double *SolA, int64_t Ndof, const double *Qw, int nq,
+            const double *CurlRef, const double *lin, const double *isNon, const double *maxB, int nmat,
+            const double *brk, int nbrk, const double *coe, int ncoe, const double *start, const double *cnt,
+            const double *coeStart, int calc_j, cudaStream_t s) {
+        int max_tag = 0;
+        MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, Tags, Ndof, mm, &max_tag, s));
+        MAG_TRY(upload_materials(lin, isNon, maxB, nmat, brk, nbrk, coe, ncoe, start, cnt, coeStart, &ms, s));
+        if (nmat < max_tag) {
+            set_error("mag_mex_jacobian: tag %d has no material entry", max_tag);
+            return MAG_E_RANGE;
+        }
+        QuadParams qp{};
+        // the Jacobian kernel takes no basis values; reuse the curl table for the slot
+        MAG_TRY(make_quad(Qw, nq, CurlRef, CurlRef, &qp, &q, s));
+        // dofs must index SolA
+        MAG_CUDA_TRY(sol.alloc(Ndof * 8));
+        MAG_CUDA_TRY(cudaMemcpyAsync(sol.p, SolA, Ndof * 8, cudaMemcpyHostToDevice, s));
+        return launch_jacobian_elems(mm.ed, sol.as<double>(), qp, ms.mp, calc_j, mm.scratch.as<double>(), s);
+    }
+};
+
 }  // namespace
 
 int mag_mex_jacobian(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
@@ -1241,32 +1290,10 @@ int mag_mex_jacobian(const double *P, int64_t Nn, const double *T, int64_t Ne, c
         set_error("mag_mex_jacobian: bad arguments");
         return MAG_E_ARG;
     }
-    MexMesh mm(s);
-    int max_tag = 0;
-    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, Tags, Ndof, mm, &max_tag, s));
-    MaterialStore ms;
-    MAG_TRY(upload_materials(lin, isNon, maxB, nmat, brk, nbrk, coe, ncoe, start, cnt, coeStart, &ms, s));
-    struct Guard {
-        MaterialStore &m;
-        double *q = nullptr;
-        ~Guard() {
-            if (m.mem) cudaFree(m.mem);
-            if (q) cudaFree(q);
-        }
-    } guard{ms};
-    if (nmat < max_tag) {
-        set_error("mag_mex_jacobian: tag %d has no material entry", max_tag);
-        return MAG_E_RANGE;
-    }
-    QuadParams qp{};
-    // the Jacobian kernel takes no basis values; reuse the curl table for the slot
-    MAG_TRY(make_quad(Qw, nq, CurlRef, CurlRef, &qp, &guard.q, s));
-    // dofs must index SolA
-    Dev sol(s);
-    MAG_CUDA_TRY(sol.alloc(Ndof * 8));
-    MAG_CUDA_TRY(cudaMemcpyAsync(sol.p, SolA, Ndof * 8, cudaMemcpyHostToDevice, s));
-    MAG_TRY(launch_jacobian_elems(mm.ed, sol.as<double>(), qp, ms.mp, calc_j, mm.scratch.as<double>(), s));
-    return mex_download(mm, Ne, calc_j, I, J, V, R_idx, R_val, s);
+    MexJacobian mj(s);
+    MAG_TRY(mj.run(P, Nn, T, Ne, Dofs, Signs, Tags, SolA, Ndof, Qw, nq, CurlRef, lin, isNon, maxB, nmat, brk,
+                   nbrk, coe, ncoe, start, cnt, coeStart, calc_j, s));
+    return mex_download(mj.mm, Ne, calc_j, I, J, V, R_idx, R_val, s);
 }
 
 int mag_mex_curl_curl(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
@@ -1319,6 +1346,313 @@ int mag_mex_mass(const double *P, int64_t Nn, const double *T, int64_t Ne, const
     if (rc == MAG_OK) rc = mex_download(mm, Ne, 1, I, J, V, nullptr, nullptr, s);
     cudaFree(dq);
     return rc;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int mag_mex_source(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                   const double *Signs, const double *Js, const double *Qw, int nq, const double *ValRef,
+                   double *I, double *V) {
+    cudaStream_t s = nullptr;
+    if (Ne == 0) return MAG_OK;
+    if (!Js || !I || !V) {
+        set_error("mag_mex_source: bad arguments");
+        return MAG_E_ARG;
+    }
+    MexMesh mm(s);
+    int max_tag = 0;
+    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, (int64_t)1 << 31, mm, &max_tag, s));
+    QuadParams qp{};
+    double *dq = nullptr;
+    MAG_TRY(make_quad(Qw, nq, ValRef, ValRef, &qp, &dq, s));
+    Dev js(s), out(s);
+    int rc = js.alloc(Ne * 24) == cudaSuccess && out.alloc(Ne * 96) == cudaSuccess ? MAG_OK : MAG_E_NOMEM;
+    if (rc == MAG_OK && cudaMemcpyAsync(js.p, Js, Ne * 24, cudaMemcpyHostToDevice, s) != cudaSuccess) rc = MAG_E_CUDA;
+    if (rc == MAG_OK) rc = launch_source_elems(mm.ed, js.as<double>(), qp, mm.scratch.as<double>(), s);
+    double *dI = out.as<double>(), *dV = dI + 6 * Ne;
+    if (rc == MAG_OK)
+        rc = launch_to_triplets(mm.scratch.as<double>(), mm.dofs.as<int32_t>(), Ne, 0, nullptr, nullptr, nullptr,
+                                dI, dV, s);
+    if (rc == MAG_OK && (cudaMemcpyAsync(I, dI, Ne * 48, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                         cudaMemcpyAsync(V, dV, Ne * 48, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                         cudaStreamSynchronize(s) != cudaSuccess))
+        rc = MAG_E_CUDA;
+    cudaFree(dq);
+    return rc;
+}
+
+int mag_mex_winding(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                    const double *Signs, const double *Tags, double CoilID, const double *DirField,
+                    const double *UniDir, double Scale, const double *Qw, int nq, const double *ValRef, double *I,
+                    double *V) {
+    cudaStream_t s = nullptr;
+    if (Ne == 0) return MAG_OK;
+    if (!Tags || (!DirField && !UniDir) || !I || !V) {
+        set_error("mag_mex_winding: bad arguments");
+        return MAG_E_ARG;
+    }
+    MexMesh mm(s);
+    int max_tag = 0;
+    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, Tags, (int64_t)1 << 31, mm, &max_tag, s));
+    QuadParams qp{};
+    double *dq = nullptr;
+    MAG_TRY(make_quad(Qw, nq, ValRef, ValRef, &qp, &dq, s));
+    Dev field(s), out(s);
+    int rc = out.alloc(Ne * 96) == cudaSuccess ? MAG_OK : MAG_E_NOMEM;
+    if (rc == MAG_OK && DirField) {
+        rc = field.alloc(Ne * 24) == cudaSuccess ? MAG_OK : MAG_E_NOMEM;
+        if (rc == MAG_OK && cudaMemcpyAsync(field.p, DirField, Ne * 24, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            rc = MAG_E_CUDA;
+    }
+    const double zero[3] = {0.0, 0.0, 0.0};
+    // (int)CoilID as the reference compares it; no tag of the mesh lies outside 1..255
+    const int coil = (CoilID > -2147483648.0 && CoilID < 2147483648.0) ? (int)CoilID : -1;
+    double *dI = out.as<double>(), *dV = dI + 6 * Ne;
+    if (rc == MAG_OK)
+        rc = launch_winding_elems(mm.ed, coil, DirField ? field.as<double>() : nullptr, UniDir ? UniDir : zero,
+                                  Scale, qp, nullptr, dI, dV, s);
+    if (rc == MAG_OK && (cudaMemcpyAsync(I, dI, Ne * 48, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                         cudaMemcpyAsync(V, dV, Ne * 48, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                         cudaStreamSynchronize(s) != cudaSuccess))
+        rc = MAG_E_CUDA;
+    cudaFree(dq);
+    return rc;
+}
+
+}  // extern "C"
+
+// ---- MATLAB sparse results of the MEX-compatible assemblies -----------------------
+
+struct mag_sparse {
+    int64_t n = 0, nnz = 0;
+    int64_t *rp = nullptr;  // [n+1] column pointers
+    int32_t *ci = nullptr;  // [nnz] row indices, ascending per column
+    double *v = nullptr;    // [nnz]
+};
+
+namespace mag {
+namespace {
+
+// Transpose each element's 6x6 block in place (the residual slot stays). Summed by the
+// row reduction, the transposed blocks give the CSR of V^T, which is the
+// compressed-column storage of sparse(I, J, V): bit-exact also where the nonlinear
+// term 2 dnu (B.C_i)(B.C_j), evaluated left to right, differs from its transpose in
+// the last bit.
+__global__ void k_transpose_blocks(double *__restrict__ scratch, int64_t ne) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    double *b = scratch + e * kScratchPerElem;
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int j = i + 1; j < 6; j++) {
+            const double t = b[i * kScratchStride + j];
+            b[i * kScratchStride + j] = b[j * kScratchStride + i];
+            b[j * kScratchStride + i] = t;
+        }
+}
+
+__global__ void k_i32_to_u64(const int32_t *__restrict__ a, int64_t n, uint64_t *__restrict__ b) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (uint64_t)(uint32_t)a[i];
+}
+
+}  // namespace
+}  // namespace mag
+
+namespace {
+
+void destroy_sparse(mag_sparse *sp) {
+    if (!sp) return;
+    if (sp->rp) cudaFree(sp->rp);
+    if (sp->ci) cudaFree(sp->ci);
+    if (sp->v) cudaFree(sp->v);
+    delete sp;
+}
+
+int empty_sparse(int64_t ndof, mag_sparse **out) {
+    mag_sparse *sp = new (std::nothrow) mag_sparse();
+    if (!sp) return MAG_E_NOMEM;
+    sp->n = ndof;
+    if (cudaMalloc(&sp->rp, (ndof + 1) * 8) != cudaSuccess || cudaMemset(sp->rp, 0, (ndof + 1) * 8) != cudaSuccess) {
+        destroy_sparse(sp);
+        set_error("mex sparse: out of device memory");
+        return MAG_E_NOMEM;
+    }
+    *out = sp;
+    return MAG_OK;
+}
+
+// sparse(I, J, V, ndof, ndof) (and, when h_res is given, full(sparse(R_idx, 1, R_val, ndof, 1))
+// into h_res) from the element blocks in mm.scratch: the mesh's CSR pattern, the
+// fixed-order row reduction over transposed blocks, then MATLAB's storage rule
+// (no explicit zeros). Missing dofs (0 in Dofs) contribute nothing, as the
+// (I > 0) & (J > 0) filter of Assembler.m:37,52,71,205 drops them.
+int mex_to_sparse(MexMesh &mm, int64_t Ne, int64_t ndof, bool with_matrix, double *h_res, mag_sparse **out,
+                  cudaStream_t s) {
+    PatternBuffers pat;
+    struct PatGuard {
+        PatternBuffers &p;
+        ~PatGuard() { free_pattern(&p, nullptr); }
+    } pg{pat};
+    MAG_TRY(build_pattern(mm.dofs.as<int32_t>(), Ne, ndof, &pat, s));
+    const RowPlan rows{pat.row_ptr, pat.inc_ptr, pat.inc_elem, pat.inc_pos, ndof, pat.wide};
+    Dev vals(s), rp64(s), res(s);
+    if (with_matrix) {
+        k_transpose_blocks<<<grid(Ne), kB, 0, s>>>(mm.scratch.as<double>(), Ne);
+        MAG_CUDA_TRY(vals.alloc(pat.nnz * 8));
+        MAG_CUDA_TRY(rp64.alloc((ndof + 1) * 8));
+    }
+    if (h_res) MAG_CUDA_TRY(res.alloc(ndof * 8));
+    MAG_TRY(launch_rows_reduce(rows, pat.max_row, mm.scratch.as<double>(), with_matrix ? vals.as<double>() : nullptr,
+                               h_res ? res.as<double>() : nullptr, s));
+    if (h_res) {
+        MAG_CUDA_TRY(cudaMemcpyAsync(h_res, res.p, ndof * 8, cudaMemcpyDeviceToHost, s));
+        MAG_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    if (!with_matrix) return MAG_OK;
+    k_i32_to_i64<<<grid(ndof + 1), kB, 0, s>>>(pat.row_ptr, ndof + 1, rp64.as<int64_t>());
+    mag_sparse *sp = new (std::nothrow) mag_sparse();
+    if (!sp) return MAG_E_NOMEM;
+    sp->n = ndof;
+    const size_t nz = pat.nnz > 0 ? (size_t)pat.nnz : 1;
+    if (cudaMalloc(&sp->rp, (ndof + 1) * 8) != cudaSuccess || cudaMalloc(&sp->ci, nz * 4) != cudaSuccess ||
+        cudaMalloc(&sp->v, nz * 8) != cudaSuccess) {
+        destroy_sparse(sp);
+        set_error("mex sparse: out of device memory");
+        return MAG_E_NOMEM;
+    }
+    int rc = csr_drop_zeros(rp64.as<int64_t>(), pat.col_idx, vals.as<double>(), ndof, sp->rp, sp->ci, sp->v,
+                            &sp->nnz, s);
+    if (rc != MAG_OK) {
+        destroy_sparse(sp);
+        return rc;
+    }
+    *out = sp;
+    return MAG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mag_mex_jacobian_sparse(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                            const double *Signs, const double *Tags, const double *SolA, int64_t Ndof,
+                            const double *Qw, int nq, const double *CurlRef, const double *lin,
+                            const double *isNon, const double *maxB, int nmat, const double *brk, int nbrk,
+                            const double *coe, int ncoe, const double *start, const double *cnt,
+                            const double *coeStart, int calc_j, mag_sparse **J_out, double *R) {
+    cudaStream_t s = nullptr;
+    if (J_out) *J_out = nullptr;
+    if (!SolA || Ndof <= 0 || !R || (calc_j && !J_out)) {
+        set_error("mag_mex_jacobian_sparse: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (Ne == 0) {
+        std::memset(R, 0, Ndof * 8);
+        return calc_j ? empty_sparse(Ndof, J_out) : MAG_OK;
+    }
+    if (!Tags) {
+        set_error("mag_mex_jacobian_sparse: bad arguments");
+        return MAG_E_ARG;
+    }
+    MexJacobian mj(s);
+    MAG_TRY(mj.run(P, Nn, T, Ne, Dofs, Signs, Tags, SolA, Ndof, Qw, nq, CurlRef, lin, isNon, maxB, nmat, brk,
+                   nbrk, coe, ncoe, start, cnt, coeStart, calc_j, s));
+    return mex_to_sparse(mj.mm, Ne, Ndof, calc_j != 0, R, J_out, s);
+}
+
+int mag_mex_curl_curl_sparse(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                             const double *Signs, const double *Nu, const double *Qw, int nq,
+                             const double *CurlRef, int64_t Ndof, mag_sparse **out) {
+    cudaStream_t s = nullptr;
+    if (out) *out = nullptr;
+    if (!out || Ndof <= 0 || (Ne > 0 && !Nu)) {
+        set_error("mag_mex_curl_curl_sparse: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (Ne == 0) return empty_sparse(Ndof, out);
+    MexMesh mm(s);
+    int max_tag = 0;
+    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, Ndof, mm, &max_tag, s));
+    QuadParams qp{};
+    double *dq = nullptr;
+    MAG_TRY(make_quad(Qw, nq, CurlRef, CurlRef, &qp, &dq, s));
+    Dev nu(s);
+    int rc = nu.alloc(Ne * 8) == cudaSuccess ? MAG_OK : MAG_E_NOMEM;
+    if (rc == MAG_OK && cudaMemcpyAsync(nu.p, Nu, Ne * 8, cudaMemcpyHostToDevice, s) != cudaSuccess) rc = MAG_E_CUDA;
+    if (rc == MAG_OK) rc = launch_stiffness_elems(mm.ed, nu.as<double>(), qp, mm.scratch.as<double>(), s);
+    if (rc == MAG_OK) rc = mex_to_sparse(mm, Ne, Ndof, true, nullptr, out, s);
+    cudaFree(dq);
+    return rc;
+}
+
+int mag_mex_mass_sparse(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                        const double *Signs, const double *Coeffs, int64_t ncoeffs, const double *Qw, int nq,
+                        const double *ValRef, int64_t Ndof, mag_sparse **out) {
+    cudaStream_t s = nullptr;
+    if (out) *out = nullptr;
+    if (!out || Ndof <= 0) {
+        set_error("mag_mex_mass_sparse: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (Ne == 0) return empty_sparse(Ndof, out);
+    MexMesh mm(s);
+    int max_tag = 0;
+    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, Ndof, mm, &max_tag, s));
+    QuadParams qp{};
+    double *dq = nullptr;
+    MAG_TRY(make_quad(Qw, nq, ValRef, ValRef, &qp, &dq, s));
+    Dev sg(s);
+    const double *dsig = nullptr;
+    int rc = MAG_OK;
+    if (Coeffs && ncoeffs == Ne) {  // otherwise sigma = 1 (assemble_mass_kernel_mex.cpp:155)
+        rc = sg.alloc(Ne * 8) == cudaSuccess ? MAG_OK : MAG_E_NOMEM;
+        if (rc == MAG_OK && cudaMemcpyAsync(sg.p, Coeffs, Ne * 8, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            rc = MAG_E_CUDA;
+        dsig = sg.as<double>();
+    }
+    if (rc == MAG_OK) rc = launch_mass_elems(mm.ed, dsig, qp, mm.scratch.as<double>(), s);
+    if (rc == MAG_OK) rc = mex_to_sparse(mm, Ne, Ndof, true, nullptr, out, s);
+    cudaFree(dq);
+    return rc;
+}
+
+int mag_sparse_info(const mag_sparse *sp, int64_t *n, int64_t *nnz) {
+    if (!sp) {
+        set_error("mag_sparse_info: null handle");
+        return MAG_E_ARG;
+    }
+    if (n) *n = sp->n;
+    if (nnz) *nnz = sp->nnz;
+    return MAG_OK;
+}
+
+int mag_sparse_copy(const mag_sparse *sp, uint64_t *jc, uint64_t *ir, double *pr) {
+    if (!sp || !jc || (sp->nnz > 0 && (!ir || !pr))) {
+        set_error("mag_sparse_copy: bad arguments");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = nullptr;
+    // column pointers are non-negative: the int64 bits are the mwIndex bits
+    MAG_CUDA_TRY(cudaMemcpyAsync(jc, sp->rp, (sp->n + 1) * 8, cudaMemcpyDeviceToHost, s));
+    if (sp->nnz > 0) {
+        Dev wide(s);
+        MAG_CUDA_TRY(wide.alloc(sp->nnz * 8));
+        k_i32_to_u64<<<grid(sp->nnz), kB, 0, s>>>(sp->ci, sp->nnz, wide.as<uint64_t>());
+        MAG_CUDA_TRY(cudaMemcpyAsync(ir, wide.p, sp->nnz * 8, cudaMemcpyDeviceToHost, s));
+        MAG_CUDA_TRY(cudaMemcpyAsync(pr, sp->v, sp->nnz * 8, cudaMemcpyDeviceToHost, s));
+        MAG_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    MAG_CUDA_TRY(cudaStreamSynchronize(s));
+    return MAG_OK;
+}
+
+int mag_sparse_destroy(mag_sparse *sp) {
+    destroy_sparse(sp);
+    return MAG_OK;
 }
 
 }  // extern "C"

@@ -132,6 +132,17 @@ class AssemblyPlan:
         _lib.check(self._lib.mag_assemble_source(self._h, _ptr(js), _ptr(out), _lib.stream_ptr(stream)))
         return out
 
+    def winding(self, coil_id: int, direction=None, scale: float = 1.0, dir_field=None, out=None, stream=None):
+        """Coil current vector of the elements tagged coil_id (mag_assemble_winding):
+        dir_field [Ne, 3] on the device, else the uniform host direction."""
+        out = self.new_vector() if out is None else out
+        d = None if direction is None else np.ascontiguousarray(np.asarray(direction, dtype=np.float64).ravel()[:3])
+        if dir_field is None and (d is None or d.size != 3):
+            raise ValueError("winding needs a 3-vector direction or an [Ne, 3] direction field")
+        _lib.check(self._lib.mag_assemble_winding(self._h, int(coil_id), _ptr(dir_field), _lib.dptr(d),
+                                                  float(scale), _ptr(out), _lib.stream_ptr(stream)))
+        return out
+
     def element_b(self, sol, want_vec: bool = True, stream=None):
         b = torch.empty((self.num_elements, 3), dtype=torch.float64, device="cuda") if want_vec else None
         bsq = torch.empty(self.num_elements, dtype=torch.float64, device="cuda")

@@ -158,6 +158,17 @@ class Port(_Lib):
                                _d(qw), C.c_int(qw.size), _d(val), _d(I), _d(V))
         return I, V
 
+    def winding(self, m: MexInputs, coil_id, dir_field, uni_dir, scale, qw, val):
+        """assemble_winding_kernel_mex.cpp:13-127; dir_field [Ne x 3] or None (uniform direction)."""
+        ne = m.ne
+        I, V = np.zeros(6 * ne), np.zeros(6 * ne)
+        qw, val, ud = _f64(qw), _f64(val), _f64(uni_dir)
+        df = None if dir_field is None else _f64(dir_field)
+        self.lib.oracle_winding(_d(m.P), _d(m.T), C.c_int64(ne), _d(m.Dofs), _d(m.Signs), _d(m.Tags),
+                                C.c_double(coil_id), _d(df), _d(ud), C.c_double(scale), _d(qw),
+                                C.c_int(qw.size), _d(val), _d(I), _d(V))
+        return I, V
+
     def hbfem(self, m: MexInputs, sol, D, P, qw, curl, packed, calc_j=True, scalings=None):
         """assemble_hbfem_kernel_mex restated with the coefficient offsets passed.
 
@@ -278,6 +289,19 @@ class RefMex(_Lib):
         rc = self.lib.ref_source(_d(m.P), C.c_size_t(m.nn), _d(m.T), C.c_size_t(ne), _d(m.Dofs),
                                  _d(m.Signs), _d(js), _d(qw), C.c_size_t(qw.size), _d(val),
                                  _d(I), _d(V), C.byref(secs))
+        self._check(rc)
+        self.last_seconds = secs.value
+        return I, V
+
+    def winding(self, m: MexInputs, coil_id, dir_field, uni_dir, scale, qw, val):
+        ne = m.ne
+        I, V = np.empty(6 * ne), np.empty(6 * ne)
+        qw, val, ud = _f64(qw), _f64(val), _f64(uni_dir)
+        df = None if dir_field is None else _f64(dir_field)
+        secs = C.c_double(0)
+        rc = self.lib.ref_winding(_d(m.P), C.c_size_t(m.nn), _d(m.T), C.c_size_t(ne), _d(m.Dofs), _d(m.Signs),
+                                  _d(m.Tags), C.c_double(coil_id), _d(df), _d(ud), C.c_double(scale), _d(qw),
+                                  C.c_size_t(qw.size), _d(val), _d(I), _d(V), C.byref(secs))
         self._check(rc)
         self.last_seconds = secs.value
         return I, V

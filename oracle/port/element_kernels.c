@@ -298,6 +298,47 @@ void oracle_source(const double *P, const double *T, int64_t Ne, const double *D
     }
 }
 
+/* Winding (coil current) vector element kernel, src/mex/assemble_winding_kernel_mex.cpp:13-127.
+ * Elements whose tag is not the coil's give I = V = 0 (:54-61); the others use the
+ * per-element direction DirField[3e..3e+2] or, when DirField is NULL, UniDir (:78-87),
+ * scaled by Scale (:90-92), mapped by J^{-1} (:96) and integrated against the reference
+ * basis without the source kernel's 1e-12 cut-off (:99-114). */
+void oracle_winding(const double *P, const double *T, int64_t Ne, const double *Dofs,
+                    const double *Signs, const double *Tags, double CoilID, const double *DirField,
+                    const double *UniDir, double Scale, const double *Qw, int nq, const double *ValRef,
+                    double *I, double *V) {
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < Ne; e++) {
+        if ((int)Tags[e] != (int)CoilID) {
+            for (int i = 0; i < 6; i++) I[6 * e + i] = V[6 * e + i] = 0.0;
+            continue;
+        }
+        double v[4][3];
+        mat3 m, inv;
+        gather_vertices(P, T, e, v);
+        double det = edge_matrix(v, &m);
+        double adet = fabs(det);
+        inverse3(&m, det, &inv);
+        const double *d = DirField ? DirField + 3 * e : UniDir;
+        double jp[3] = {d[0] * Scale, d[1] * Scale, d[2] * Scale};
+        double jr[3];
+        apply(&inv, jp, jr);
+        double f[6] = {0, 0, 0, 0, 0, 0};
+        for (int q = 0; q < nq; q++) {
+            double w = Qw[q] * adet;
+            for (int i = 0; i < 6; i++) {
+                double r[3];
+                ref_vec(ValRef, i, q, r);
+                f[i] += dot3(jr, r) * w;
+            }
+        }
+        for (int i = 0; i < 6; i++) {
+            I[6 * e + i] = (double)(int64_t)Dofs[6 * e + i];
+            V[6 * e + i] = f[i] * Signs[6 * e + i];
+        }
+    }
+}
+
 /* Harmonic-balance element kernel, restating src/mex/assemble_hbfem_kernel_mex.cpp:26-258
  * with the coefficient offsets passed (the gateway leaves them unset). For each element:
  * the signed harmonic edge values A_h (re, im), the time samples

@@ -51,6 +51,12 @@ void oracle_mass(const double *P, const double *T, int64_t Ne, const double *Dof
                  const double *Signs, const double *Coeffs, int64_t ncoeff, const double *Qw, int nq,
                  const double *ValRef, double *I, double *J, double *V);
 
+/* Winding vector element kernel, src/mex/assemble_winding_kernel_mex.cpp:13-127.
+ * DirField [3 x Ne] or NULL (then UniDir [3]). */
+void oracle_winding(const double *P, const double *T, int64_t Ne, const double *Dofs,
+                    const double *Signs, const double *Tags, double CoilID, const double *DirField,
+                    const double *UniDir, double Scale, const double *Qw, int nq, const double *ValRef,
+                    double *I, double *V);
 /* Source vector element kernel, src/mex/assemble_source_kernel_mex.cpp:16-114. */
 void oracle_source(const double *P, const double *T, int64_t Ne, const double *Dofs,
                    const double *Signs, const double *Js, const double *Qw, int nq,

@@ -7,9 +7,11 @@
  *   src/mex/assemble_curl_curl_kernel_mex.cpp  -> ref_curl_curl_mexFunction
  *   src/mex/assemble_mass_kernel_mex.cpp       -> ref_mass_mexFunction
  *   src/mex/assemble_source_kernel_mex.cpp     -> ref_source_mexFunction
+ *   src/mex/assemble_hbfem_kernel_mex.cpp      -> ref_hbfem_mexFunction
+ *   src/mex/assemble_winding_kernel_mex.cpp    -> ref_winding_mexFunction
  * This file implements the mex.h stand-in (oracle/mex_shim/mex.h) and exposes
  * plain C entry points that build the mxArray argument lists exactly as
- * Assembler.m does (Assembler.m:33,48,67,87,199-202) and hand the MEX outputs
+ * Assembler.m does (Assembler.m:33,48,67,87,157-160,199-202) and hand the MEX outputs
  * back in caller-owned buffers. Nothing here is shipped or measured as product.
  */
 #include "mex.h"
@@ -74,6 +76,7 @@ void ref_curl_curl_mexFunction(int, mxArray *[], int, const mxArray *[]);
 void ref_mass_mexFunction(int, mxArray *[], int, const mxArray *[]);
 void ref_source_mexFunction(int, mxArray *[], int, const mxArray *[]);
 void ref_hbfem_mexFunction(int, mxArray *[], int, const mxArray *[]);
+void ref_winding_mexFunction(int, mxArray *[], int, const mxArray *[]);
 
 const char *ref_last_error(void) { return g_err_msg; }
 
@@ -181,6 +184,22 @@ int ref_source(const double *P, size_t Nn, const double *T, size_t Ne, const dou
     double *outs[2] = {I, V};
     size_t outn[2] = {Ne * 6, Ne * 6};
     return run(ref_source_mexFunction, 2, 7, in, outs, outn, seconds);
+}
+
+/* [I,V] = assemble_winding_kernel_mex(P,T,Dofs,Signs,Tags,CoilID,DirField,UniDir,Scale,Qw,ValRef),
+ * Assembler.m:157-166. DirField NULL is passed as the empty []. */
+int ref_winding(const double *P, size_t Nn, const double *T, size_t Ne, const double *Dofs,
+                const double *Signs, const double *Tags, double CoilID, const double *DirField,
+                const double *UniDir, double Scale, const double *Qw, size_t nq, const double *ValRef,
+                double *I, double *V, double *seconds) {
+    mxArray in[11] = {wrap(P, 3, Nn),       wrap(T, 4, Ne),          wrap(Dofs, 6, Ne),
+                      wrap(Signs, 6, Ne),   wrap(Tags, 1, Ne),       wrap(&CoilID, 1, 1),
+                      DirField ? wrap(DirField, 3, Ne) : wrap(nullptr, 0, 0),
+                      wrap(UniDir, 3, 1),   wrap(&Scale, 1, 1),      wrap(Qw, 1, nq),
+                      wrap(ValRef, 18, nq)};
+    double *outs[2] = {I, V};
+    size_t outn[2] = {Ne * 6, Ne * 6};
+    return run(ref_winding_mexFunction, 2, 11, in, outs, outn, seconds);
 }
 
 /* [I,J,V,R_rows,R_cols,R_re,R_im] = assemble_hbfem_kernel_mex(22 args)

@@ -55,6 +55,13 @@ def run_case(name, P, T0, tags, matlib, sol_scale, seed, sigma, js_iron):
     Is, Vs = ref.source(m, js, qw, val)
     out.update(cc_nu=nu, cc_V=Vk, mass_sigma=sig, mass_V=Vm, mass1_V=Vm1, src_js=js, src_I=Is,
                src_V=Vs)
+    # winding vector of the iron region: uniform direction, then a per-element direction field
+    wdir, wscale = np.array([0.3, -0.5, 0.8]), 250.0 / 2.5e-3
+    wfield = rng.normal(0.0, 1.0, (T0.shape[0], 3))
+    Iu, Vu = ref.winding(m, float(synth.IRON), None, wdir, wscale, qw, val)
+    If, Vf = ref.winding(m, float(synth.IRON), wfield, wdir, wscale, qw, val)
+    out.update(win_coil=np.array(float(synth.IRON)), win_dir=wdir, win_scale=np.array(wscale),
+               win_field=wfield, win_u_I=Iu, win_u_V=Vu, win_f_I=If, win_f_V=Vf)
     np.savez_compressed(
         os.path.join(HERE, f"{name}.npz"), P=P, T0=T0, tags=tags, edges=edges, t2e=t2e, sign=sign,
         sol=sol, qw=qw, curl=curl, val=val, mat_lin=pk.lin, mat_isnon=pk.is_non, mat_maxb=pk.max_b,

@@ -11,14 +11,35 @@ GXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 GCC = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
 
 
-@pytest.mark.parametrize("src", sorted(glob.glob(os.path.join(ROOT, "magpackage_b200", "mex", "*.cpp"))))
+GATEWAYS = sorted(glob.glob(os.path.join(ROOT, "magpackage_b200", "mex", "*.cpp")))
+
+
+@pytest.mark.parametrize("src", GATEWAYS)
 def test_mex_gateways_compile(src):
-    """Each gateway compiles against a mex.h (the oracle's stand-in here; MATLAB's own
+    """Each gateway compiles against a mex.h (the tests' stand-in here; MATLAB's own
     header in a real build) and the C ABI header."""
     out = subprocess.run([GXX, "-std=c++11", "-fsyntax-only", "-Wall", "-Werror",
-                          "-I" + os.path.join(ROOT, "oracle", "mex_shim"), "-I" + os.path.join(ROOT, "include"),
+                          "-I" + os.path.join(ROOT, "tests", "mex_host"), "-I" + os.path.join(ROOT, "include"),
                           src], capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
+
+
+@pytest.mark.parametrize("name,nargs,msg", [
+    ("assemble_jacobian_kernel_mex", 16, "Expected 17 inputs (18 with the sparse-output flag)."),
+    ("assemble_jacobian_kernel_mex", 19, "Expected 17 inputs (18 with the sparse-output flag)."),
+    ("assemble_curl_curl_kernel_mex", 6, "Expected 7 inputs (8 with Ndof)."),
+    ("assemble_mass_kernel_mex", 9, "Expected 7 inputs (8 with Ndof)."),
+    ("assemble_source_kernel_mex", 8, "Expected 7 inputs."),
+    ("assemble_winding_kernel_mex", 10, "Expected 11 inputs."),
+])
+def test_gateway_rejects_argument_count(tmp_path, name, nargs, msg):
+    """The gateways link against libmagasm and raise MagPackage:Args, as the reference's
+    do, before any device work (runs without a GPU)."""
+    from mex_host.gateway import Gateway, GatewayError, build
+
+    gw = Gateway(build(name, tmp_path))
+    with pytest.raises(GatewayError, match="MagPackage:Args: " + msg.replace("(", r"\(").replace(")", r"\)")):
+        gw(5, *([0.0] * nargs))
 
 
 def test_harness_compiles(tmp_path):

@@ -33,6 +33,10 @@ def test_port_matches_golden(oracle_port, name):
     assert bits_equal(Vm1, d["mass1_V"])
     Is, Vs = oracle_port.source(m, d["src_js"], d["qw"], d["val"])
     assert bits_equal(Is, d["src_I"]) and bits_equal(Vs, d["src_V"])
+    for field, key in ((None, "u"), (d["win_field"], "f")):
+        Iw, Vw = oracle_port.winding(m, float(d["win_coil"]), field, d["win_dir"], float(d["win_scale"]), d["qw"],
+                                     d["val"])
+        assert bits_equal(Iw, d[f"win_{key}_I"]) and bits_equal(Vw, d[f"win_{key}_V"])
 
 
 def test_unit_tet_known_answer(oracle_port):
@@ -144,6 +148,14 @@ def test_port_matches_live_reference(oracle_port, oracle_ref):
     assert bits_equal(oracle_ref.mass(m, sig, qw, val)[2], oracle_port.mass(m, sig, qw, val)[2])
     js = np.random.default_rng(5).normal(size=(mesh.num_elements, 3))
     assert bits_equal(oracle_ref.source(m, js, qw, val)[1], oracle_port.source(m, js, qw, val)[1])
+    # winding: coil region present or absent, uniform or per-element direction, missing dofs
+    m.Dofs[::7, 2] = 0.0
+    field = np.random.default_rng(6).normal(size=(mesh.num_elements, 3))
+    for coil in (float(synth.ALUMINIUM), float(synth.IRON), 99.0):
+        for f in (None, field):
+            r = oracle_ref.winding(m, coil, f, (0.0, 0.6, -0.8), 4.0e5, qw, val)
+            p = oracle_port.winding(m, coil, f, (0.0, 0.6, -0.8), 4.0e5, qw, val)
+            assert bits_equal(r[0], p[0]) and bits_equal(r[1], p[1])
 
 
 def _hbfem_case(oracle_port, iron_nonlinear, n=(4, 3, 3), seed=11, harmonics=(0, 1, 3), imag=True):
