@@ -338,8 +338,9 @@ def main():
     ap.add_argument("--workload", default="jacobian_60",
                     choices=sorted(WORKLOADS) + ["batched_complex", "transient", "hbfem"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--schedule", default="shared-row-blocks",
-                    choices=["shared-row-blocks", "staged-row-blocks", "row-blocks", "l2-ring", "two-pass"],
+    ap.add_argument("--schedule", default="nz-row-blocks",
+                    choices=["shared-row-blocks", "nz-row-blocks", "staged-row-blocks", "row-blocks", "l2-ring",
+                             "two-pass"],
                     help="Jacobian assembly schedule (all give identical bits)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -382,6 +383,7 @@ def main():
     plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
     plan.set_materials(packed)
     sched_id = {"shared-row-blocks": _lib.SCHEDULE_SHARED_ROW_BLOCKS,
+                "nz-row-blocks": _lib.SCHEDULE_NZ_ROW_BLOCKS,
                 "staged-row-blocks": _lib.SCHEDULE_STAGED_ROW_BLOCKS,
                 "row-blocks": _lib.SCHEDULE_ROW_BLOCKS, "l2-ring": _lib.SCHEDULE_L2_RING,
                 "two-pass": _lib.SCHEDULE_TWO_PASS}[args.schedule]
@@ -532,7 +534,10 @@ def main():
                        "l2": "inputs larger than L2 (per-step working set > 700 MB)",
                        "parallelism": f"{world} independent instance(s)",
                        "shared_blocks": plan.info.shared_blocks, "shared_staged": plan.info.shared_staged,
-                       "schedule": {_lib.SCHEDULE_STAGED_ROW_BLOCKS: "row blocks with shared elements, the "
+                       "schedule": {_lib.SCHEDULE_NZ_ROW_BLOCKS: "row blocks with shared elements; "
+                                                                 "off-diagonal entries placed by their "
+                                                                 "incidences, one pass over the nonzeros",
+                                    _lib.SCHEDULE_STAGED_ROW_BLOCKS: "row blocks with shared elements, the "
                                                                      "block's nodes and edge values staged in "
                                                                      "shared memory first",
                                     _lib.SCHEDULE_SHARED_ROW_BLOCKS: "row blocks: one launch, no scratch, "

@@ -57,6 +57,7 @@ typedef struct {
     int64_t device_bytes;   /* memory held by the handle */
     int32_t shared_blocks;  /* row blocks of MAG_SCHEDULE_SHARED_ROW_BLOCKS (0 = not available) */
     int32_t shared_staged;  /* 1 once MAG_SCHEDULE_STAGED_ROW_BLOCKS has been selected (tables built) */
+    int32_t nz_pass;        /* 1 if MAG_SCHEDULE_NZ_ROW_BLOCKS is available for this mesh */
 } mag_mesh_info;
 
 /* Jacobian assembly schedules; all give identical bits. */
@@ -65,10 +66,15 @@ typedef struct {
 #define MAG_SCHEDULE_L2_RING 1    /* one persistent launch, scratch ring sized to stay in L2 */
 #define MAG_SCHEDULE_ROW_BLOCKS 2 /* one launch, no scratch: per-row element recompute */
 #define MAG_SCHEDULE_SHARED_ROW_BLOCKS 3 /* as 2, each block's distinct elements evaluated once in shared
-                                            memory (default; standard curl table, else runs as 2) */
+                                            memory (standard curl table, else runs as 2) */
 #define MAG_SCHEDULE_STAGED_ROW_BLOCKS 4 /* as 3, the block's distinct nodes and edge values first gathered
                                             once into shared memory (measured slower than 3 on B200); its
                                             tables are built when it is first selected */
+#define MAG_SCHEDULE_NZ_ROW_BLOCKS 5     /* as 3, each off-diagonal entry placed by its (at most two)
+                                            contributing incidences and the block's nonzeros stored in one
+                                            pass; only diagonals and residuals are summed per row (meshes
+                                            whose off-diagonal entries have more than two contributions,
+                                            e.g. repeated dofs, run as 3). The default when available */
 
 /* ---- library ------------------------------------------------------------ */
 

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libmagasm.so")
 
 MAG_OK = 0
 SCHEDULE_TWO_PASS, SCHEDULE_L2_RING, SCHEDULE_ROW_BLOCKS, SCHEDULE_SHARED_ROW_BLOCKS = 0, 1, 2, 3
-SCHEDULE_STAGED_ROW_BLOCKS = 4
+SCHEDULE_STAGED_ROW_BLOCKS, SCHEDULE_NZ_ROW_BLOCKS = 4, 5
 _ERRNAMES = {-1: "MAG_E_ARG", -2: "MAG_E_RANGE", -3: "MAG_E_GEOMETRY", -4: "MAG_E_CUDA",
              -5: "MAG_E_TIMEOUT", -6: "MAG_E_NOMEM", -7: "MAG_E_UNSUPPORTED"}
 
@@ -30,7 +30,7 @@ class MeshInfo(C.Structure):
                 ("nnz", C.c_int64), ("num_incidences", C.c_int64), ("max_row_nnz", C.c_int32),
                 ("wide_positions", C.c_int32), ("signs_derived", C.c_int32), ("schedule", C.c_int32),
                 ("fused_ring_tiles", C.c_int32), ("fused_grid", C.c_int32), ("device_bytes", C.c_int64),
-                ("shared_blocks", C.c_int32), ("shared_staged", C.c_int32)]
+                ("shared_blocks", C.c_int32), ("shared_staged", C.c_int32), ("nz_pass", C.c_int32)]
 
 
 _vp = C.c_void_p

@@ -472,9 +472,10 @@ int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t N
         free_fused_plan(&m->fused);
         cudaGetLastError();
     }
-    m->schedule = m->rowshared.shared_ok ? MAG_SCHEDULE_SHARED_ROW_BLOCKS
-                  : m->rowblock.ok        ? MAG_SCHEDULE_ROW_BLOCKS
-                                          : MAG_SCHEDULE_TWO_PASS;
+    m->schedule = m->rowshared.nz_ok       ? MAG_SCHEDULE_NZ_ROW_BLOCKS
+                  : m->rowshared.shared_ok ? MAG_SCHEDULE_SHARED_ROW_BLOCKS
+                  : m->rowblock.ok         ? MAG_SCHEDULE_ROW_BLOCKS
+                                           : MAG_SCHEDULE_TWO_PASS;
     double qw[4], curl[72], val[72];
     default_reference_data(qw, curl, val);
     rc = make_quad(qw, 4, curl, val, &m->qp, &m->d_ref, s);
@@ -508,6 +509,7 @@ int mag_mesh_get_info(const mag_mesh *m, mag_mesh_info *info) {
     info->device_bytes = m->bytes;
     info->shared_blocks = m->rowshared.shared_ok ? m->rowshared.nblocks : 0;
     info->shared_staged = m->rowshared.staged_ok;
+    info->nz_pass = m->rowshared.nz_ok;
     return MAG_OK;
 }
 
@@ -554,12 +556,19 @@ int mag_assemble_jacobian(mag_mesh *m, const double *d_sol, double *d_vals, doub
     }
     cudaStream_t s = (cudaStream_t)stream;
     const bool staged = m->schedule == MAG_SCHEDULE_STAGED_ROW_BLOCKS;
-    if ((m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || staged) && m->rowshared.shared_ok && m->qp.standard_curl) {
+    if (m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS && m->rowshared.nz_ok && m->qp.standard_curl) {
+        MAG_TRY(launch_rowblock_nz_jacobian(m->rowshared, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp, calc_j,
+                                            calc_j ? d_vals : nullptr, d_res, s));
+        return finish(s);
+    }
+    if ((m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || staged || m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS) &&
+        m->rowshared.shared_ok && m->qp.standard_curl) {
         MAG_TRY(launch_rowblock_shared_jacobian(m->rowshared, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp,
                                                 calc_j, calc_j ? d_vals : nullptr, d_res, s, staged));
         return finish(s);
     }
-    if (m->schedule == MAG_SCHEDULE_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || staged) {
+    if (m->schedule == MAG_SCHEDULE_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || staged ||
+        m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS) {
         MAG_TRY(launch_rowblock_jacobian(m->rowblock, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp, calc_j,
                                          calc_j ? d_vals : nullptr, d_res, s));
         return finish(s);
@@ -736,7 +745,8 @@ int mag_mesh_set_option(mag_mesh *m, int option, int64_t value) {
         if ((value == MAG_SCHEDULE_L2_RING && !m->fused.ok) ||
             (value == MAG_SCHEDULE_ROW_BLOCKS && !m->rowblock.ok) ||
             (value == MAG_SCHEDULE_SHARED_ROW_BLOCKS && !m->rowshared.shared_ok) ||
-            (value == MAG_SCHEDULE_STAGED_ROW_BLOCKS && !m->rowshared.staged_ok) || value < 0 || value > 4) {
+            (value == MAG_SCHEDULE_STAGED_ROW_BLOCKS && !m->rowshared.staged_ok) ||
+            (value == MAG_SCHEDULE_NZ_ROW_BLOCKS && !m->rowshared.nz_ok) || value < 0 || value > 5) {
             set_error("assembly schedule %lld is not available for this mesh", (long long)value);
             return MAG_E_UNSUPPORTED;
         }

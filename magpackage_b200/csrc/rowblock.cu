@@ -192,6 +192,58 @@ __global__ void __launch_bounds__(kBlockInc, 4) k_rowblock(RBArgs A) {
 
 // ---- shared-element variant --------------------------------------------------------
 
+// In-row positions of incidence k's six columns (kCompactMaxRow / kWideMaxRow = no dof).
+template <bool WIDE>
+__device__ __forceinline__ void inc_positions(const RowPlan &rp, int64_t k, unsigned p[6]) {
+    if (!WIDE) {
+        const uint32_t pw = rp.inc_pos[k];
+#pragma unroll
+        for (int j = 0; j < 6; j++) p[j] = (pw >> (5 * j)) & 31u;
+    } else {
+        const uint32_t w0 = rp.inc_pos[2 * k], w1 = rp.inc_pos[2 * k + 1];
+#pragma unroll
+        for (int j = 0; j < 6; j++) p[j] = (j < 4 ? (w0 >> (8 * j)) : (w1 >> (8 * (j - 4)))) & 255u;
+    }
+}
+
+// Per incidence (row order) bit j: an earlier incidence of the same row (a lower
+// element) also adds to column j's position, so this one is the second of that
+// off-diagonal entry's contributions. Sets *bad when an off-diagonal position of a row
+// has more than two contributions or a column other than the element's own edge lands
+// on the diagonal (a repeated dof), which the nonzero-pass kernel cannot place.
+template <bool WIDE>
+__global__ void __launch_bounds__(256) k_second_masks(RowPlan rp, uint8_t *__restrict__ second, int *__restrict__ bad) {
+    const int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (a >= rp.ndof) return;
+    const unsigned none = WIDE ? (unsigned)kWideMaxRow : (unsigned)kCompactMaxRow;
+    const int k0 = rp.inc_ptr[a], k1 = rp.inc_ptr[a + 1];
+    for (int k = k0; k < k1; k++) {
+        unsigned p[6];
+        inc_positions<WIDE>(rp, k, p);
+        const unsigned loc = rp.inc_elem[k] >> 29;
+        unsigned pd = p[0];
+#pragma unroll
+        for (int j = 1; j < 6; j++) pd = loc == (unsigned)j ? p[j] : pd;
+        unsigned mask = 0;
+        for (int j = 0; j < 6; j++) {
+            if ((unsigned)j == loc || p[j] == none) continue;
+            if (p[j] == pd) atomicExch(bad, 1);
+            int before = 0;
+            for (int q = k0; q < k; q++) {
+                unsigned pq[6];
+                inc_positions<WIDE>(rp, q, pq);
+                const unsigned lq = rp.inc_elem[q] >> 29;
+#pragma unroll
+                for (int i = 0; i < 6; i++) before += ((unsigned)i != lq && pq[i] == p[j]) ? 1 : 0;
+            }
+            if (before == 1) mask |= 1u << j;
+            if (before > 1) atomicExch(bad, 1);
+        }
+        second[k] = (uint8_t)mask;
+    }
+}
+
+
 // Per block: sort its (element, incidence) pairs, number the distinct elements in
 // ascending order, and record each incidence's slot. Counts above MAXE set *overflow.
 template <int BI, int MAXE>
@@ -200,7 +252,8 @@ __global__ void __launch_bounds__(BI) k_block_elems(RowPlan rp, const int32_t *_
                                                            int32_t *__restrict__ blk_k0,
                                                            int32_t *__restrict__ blk_elem,
                                                            uint16_t *__restrict__ inc_slot,
-                                                           uint32_t *__restrict__ inc_sorted, int *overflow) {
+                                                           uint32_t *__restrict__ inc_sorted,
+                                                           const uint8_t *__restrict__ second, int *overflow) {
     __shared__ unsigned long long key[BI];
     __shared__ int scan[BI];
     const int t = threadIdx.x;
@@ -240,7 +293,9 @@ __global__ void __launch_bounds__(BI) k_block_elems(RowPlan rp, const int32_t *_
         const int orig = (int)(me & 0xFF);
         const uint32_t loc = rp.inc_elem[k0 + orig] >> 29;
         inc_slot[k0 + orig] = (uint16_t)(slot | (loc << 8));
-        if (inc_sorted) inc_sorted[k0 + t] = (uint32_t)slot | loc << 8 | (uint32_t)orig << 16;
+        if (inc_sorted)
+            inc_sorted[k0 + t] = (uint32_t)slot | loc << 8 | (uint32_t)orig << 16 |
+                                 (second ? (uint32_t)second[k0 + orig] << 24 : 0u);
         if (first) blk_elem[k0 + slot] = (int32_t)(me >> 8);
     }
     if (t == 0) {
@@ -548,7 +603,7 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const in
         double bl = R.b[0];
 #pragma unroll
         for (int j = 1; j < 6; j++) bl = loc == j ? R.b[j] : bl;
-        double *out = sv + (my_inc >> 16) * kSv2;
+        double *out = sv + ((my_inc >> 16) & 0xFF) * kSv2;
         out[6] = flip(qsum_w<Q4>(nu * bl, A.qp, w0, R.adet), si);
         if (CALCJ) {
             if (R.g2 == 0.0) {
@@ -599,6 +654,202 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const in
     if (CALCJ) {
         __syncthreads();
         for (int i = tid; i < span; i += BI) A.vals[base + i] = sacc[skew(i)];
+    }
+}
+
+// ---- nonzero-pass variant ----------------------------------------------------------
+
+// Shared-memory carve-up of one block of the nonzero-pass kernel.
+template <int BI, int MAXE>
+struct NzLayout {
+    static constexpr int rec = (int)sizeof(ElemRec) * MAXE;
+    static constexpr int nzv = 16 * kNzMaxSpan;  // two slots per CSR nonzero of the block
+    static constexpr int sv = 16 * BI;           // per incidence (row order): residual, diagonal entry
+    static constexpr int rsb = 4 * MAXE;
+    static constexpr int pos = 8 * BI;           // in-row positions (2 words per incidence when wide)
+    static constexpr int roff = 2 * BI;          // per incidence: its row's first nonzero in the block
+    static constexpr int loc = BI;               // per incidence: the local edge of its row
+    static constexpr int bytes = rec + nzv + sv + rsb + pos + roff + loc + 8 * (BI + 1);
+    static_assert(rec % 16 == 0 && nzv % 16 == 0 && sv % 16 == 0, "alignment of the shared-memory carve-up");
+};
+
+// Shared-element row blocks with a nonzero pass. A1 as k_rowblock_shared. A2: one thread
+// per incidence forms its element row and writes each off-diagonal entry straight into
+// its CSR nonzero's slot (0 for the lower element, 1 for the higher: an off-diagonal
+// entry has at most two contributions, whose sum does not depend on their order), and
+// its diagonal entry and residual into per-incidence slots. B1: one thread per row sums
+// the diagonal and the residual over its incidences in ascending element order. B2: one
+// thread per nonzero stores (0 + slot 0) + slot 1, coalesced. Same bits as k_rowblock.
+template <int BI, int MAXE, int MINB, bool CALCJ, bool Q4, bool WIDE>
+__global__ void __launch_bounds__(BI, MINB) k_rowblock_nz(RBArgs A, const int32_t *__restrict__ blk_nelem,
+                                                          const int32_t *__restrict__ blk_k0,
+                                                          const int32_t *__restrict__ blk_elem,
+                                                          const uint32_t *__restrict__ inc_sorted) {
+    using L = NzLayout<BI, MAXE>;
+    extern __shared__ __align__(16) unsigned char nz_smem[];
+    ElemRec *rec = reinterpret_cast<ElemRec *>(nz_smem);
+    double2 *nzv = reinterpret_cast<double2 *>(nz_smem + L::rec);
+    double2 *sv = reinterpret_cast<double2 *>(nz_smem + L::rec + L::nzv);
+    unsigned *rsb = reinterpret_cast<unsigned *>(nz_smem + L::rec + L::nzv + L::sv);
+    uint32_t *spos = reinterpret_cast<uint32_t *>(nz_smem + L::rec + L::nzv + L::sv + L::rsb);
+    uint16_t *sroff = reinterpret_cast<uint16_t *>(nz_smem + L::rec + L::nzv + L::sv + L::rsb + L::pos);
+    uint8_t *sloc = nz_smem + L::rec + L::nzv + L::sv + L::rsb + L::pos + L::roff;
+    int *s_ip = reinterpret_cast<int *>(nz_smem + L::rec + L::nzv + L::sv + L::rsb + L::pos + L::roff + L::loc);
+    int *s_off = s_ip + (BI + 1);
+    constexpr unsigned kNone = WIDE ? (unsigned)kWideMaxRow : (unsigned)kCompactMaxRow;
+    const int tid = threadIdx.x;
+    const int a0 = A.block_row[blockIdx.x], a1 = A.block_row[blockIdx.x + 1];
+    const int k0 = blk_k0[blockIdx.x], ninc = blk_k0[blockIdx.x + 1] - k0;
+    const int nel = blk_nelem[blockIdx.x];
+    const int nrows = a1 - a0;
+    const int base = A.rp.row_ptr[a0], span = A.rp.row_ptr[a1] - base;
+    const unsigned my_inc = tid < ninc ? __ldg(inc_sorted + k0 + tid) : 0u;
+    if (CALCJ && tid < ninc) {
+        if (WIDE) {
+            spos[2 * tid] = __ldg(A.rp.inc_pos + 2 * (int64_t)(k0 + tid));
+            spos[2 * tid + 1] = __ldg(A.rp.inc_pos + 2 * (int64_t)(k0 + tid) + 1);
+        } else {
+            spos[tid] = __ldg(A.rp.inc_pos + k0 + tid);
+        }
+    }
+    // per row: first incidence and first nonzero (block-relative); per incidence: its row's
+    // first nonzero
+    for (int r = tid; r <= nrows; r += BI) {
+        const int ip = A.rp.inc_ptr[a0 + r] - k0, off = A.rp.row_ptr[a0 + r] - base;
+        s_ip[r] = ip;
+        s_off[r] = off;
+        if (CALCJ && r < nrows) {
+            const int ipn = A.rp.inc_ptr[a0 + r + 1] - k0;
+            for (int k = ip; k < ipn; k++) sroff[k] = (uint16_t)off;
+        }
+    }
+    if (CALCJ)
+        for (int i = tid; i < span; i += BI) nzv[i] = make_double2(0.0, 0.0);
+    // phase A1: one thread per distinct element (the plan keeps nel <= MAXE)
+    if (tid < nel && tid < MAXE) {
+        const int64_t e = blk_elem[k0 + tid];
+        const int4 tt = A.m.tet[e];
+        int d[6];
+        load_dofs(A.m.dofs, e, d);
+        const unsigned sb = A.m.signbits ? A.m.signbits[e] : derived_signs(tt);
+        const int tag = A.m.tags[e];
+        Geo g;
+        geometry(A.m.xyz, tt, g);
+        double a[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) a[i] = d[i] >= 0 ? flip(__ldg(A.sol + d[i]), (sb >> i) & 1) : 0.0;
+        double C[6][3];
+        curls_standard(g, C);
+        double B[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double v = a[0] * C[0][c];
+#pragma unroll
+            for (int i = 1; i < 6; i++) v = v + a[i] * C[i][c];
+            B[c] = v;
+        }
+        double nu, dnu;
+        material_eval(A.mp, tag, dot3(B, B), nu, dnu);
+        ElemRec &R = rec[tid];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) R.J[3 * r + c] = g.J[r][c];
+        R.r2 = 2.0 * g.rdet;
+#pragma unroll
+        for (int j = 0; j < 6; j++) R.b[j] = dot3(B, C[j]);
+        R.nu = nu;
+        R.g2 = 2.0 * dnu;
+        R.adet = g.adet;
+        rsb[tid] = sb;
+    }
+    __syncthreads();
+    // phase A2: one thread per incidence, walking them in element order
+    if (tid < ninc) {
+        const ElemRec &R = rec[my_inc & 0xFF];
+        const int loc = (int)((my_inc >> 8) & 0xFF);
+        const int k = (int)((my_inc >> 16) & 0xFF);
+        const unsigned second = my_inc >> 24;
+        const unsigned sb = rsb[my_inc & 0xFF];
+        Geo g;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) g.J[r][c] = R.J[3 * r + c];
+        g.rdet = 0.5 * R.r2;  // exact: curls_standard forms 2 * rdet again
+        g.adet = R.adet;
+        double C[6][3];
+        curls_standard(g, C);
+        const unsigned si = (sb >> loc) & 1;
+        const double w0 = A.qp.qw[0] * R.adet, nu = R.nu;
+        double Cl[3];
+        pick(C, loc, Cl);
+        double bl = R.b[0];
+#pragma unroll
+        for (int j = 1; j < 6; j++) bl = loc == j ? R.b[j] : bl;
+        const double rv = flip(qsum_w<Q4>(nu * bl, A.qp, w0, R.adet), si);
+        double dv = 0.0;
+        if (CALCJ) {
+            double v[6];
+            if (R.g2 == 0.0) {
+#pragma unroll
+                for (int j = 0; j < 6; j++)
+                    v[j] = flip(qsum_w<Q4>(nu * dot3(Cl, C[j]), A.qp, w0, R.adet), si ^ ((sb >> j) & 1));
+            } else {
+                const double gl = R.g2 * bl;
+#pragma unroll
+                for (int j = 0; j < 6; j++)
+                    v[j] = flip(qsum_w<Q4>(nu * dot3(Cl, C[j]) + gl * R.b[j], A.qp, w0, R.adet), si ^ ((sb >> j) & 1));
+            }
+            unsigned p[6];
+            if (!WIDE) {
+                const uint32_t pw = spos[k];
+#pragma unroll
+                for (int j = 0; j < 6; j++) p[j] = (pw >> (5 * j)) & 31u;
+            } else {
+                const uint32_t w0p = spos[2 * k], w1p = spos[2 * k + 1];
+#pragma unroll
+                for (int j = 0; j < 6; j++) p[j] = (j < 4 ? (w0p >> (8 * j)) : (w1p >> (8 * (j - 4)))) & 255u;
+            }
+            double *slots = reinterpret_cast<double *>(nzv) + 2 * (int)sroff[k];
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                if (j == loc) dv = v[j];
+                else if (p[j] != kNone) slots[2 * p[j] + ((second >> j) & 1)] = v[j];
+            }
+            sloc[k] = (uint8_t)loc;
+        }
+        sv[k] = make_double2(rv, dv);
+    }
+    __syncthreads();
+    // phase B1: one thread per row, the diagonal and the residual in ascending element order
+    for (int r = tid; r < nrows; r += BI) {
+        const int i0 = s_ip[r], i1 = s_ip[r + 1];
+        double racc = 0.0, dacc = 0.0;
+        for (int k = i0; k < i1; k++) {
+            const double2 v = sv[k];
+            racc = racc + v.x;
+            if (CALCJ) dacc = dacc + v.y;
+        }
+        A.res[a0 + r] = racc;
+        if (CALCJ && i1 > i0) {
+            const int l = sloc[i0];
+            unsigned pd;
+            if (!WIDE) {
+                pd = (spos[i0] >> (5 * l)) & 31u;
+            } else {
+                pd = (l < 4 ? (spos[2 * i0] >> (8 * l)) : (spos[2 * i0 + 1] >> (8 * (l - 4)))) & 255u;
+            }
+            reinterpret_cast<double *>(nzv)[2 * (s_off[r] + (int)pd)] = dacc;
+        }
+    }
+    if (CALCJ) {
+        __syncthreads();
+        // phase B2: one thread per nonzero
+        for (int i = tid; i < span; i += BI) {
+            const double2 v = nzv[i];
+            A.vals[base + i] = (0.0 + v.x) + v.y;
+        }
     }
 }
 
@@ -663,8 +914,9 @@ void build_stage(const ElemData &m, RowBlockPlan *out, cudaStream_t s) {
 int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc, bool with_shared,
                         const ElemData *stage_mesh) {
     *out = RowBlockPlan{};
-    std::vector<int32_t> ip((size_t)rp.ndof + 1);
+    std::vector<int32_t> ip((size_t)rp.ndof + 1), rpp((size_t)rp.ndof + 1);
     MAG_CUDA_TRY(cudaMemcpyAsync(ip.data(), rp.inc_ptr, ip.size() * 4, cudaMemcpyDeviceToHost, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(rpp.data(), rp.row_ptr, rpp.size() * 4, cudaMemcpyDeviceToHost, s));
     MAG_CUDA_TRY(cudaStreamSynchronize(s));
     std::vector<int32_t> starts;
     starts.reserve((size_t)(rp.ndof / 32) + 2);
@@ -691,6 +943,35 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
             cudaMalloc(&out->inc_sorted, (size_t)(ninc > 0 ? ninc : 1) * 4) != cudaSuccess)
             with_shared = false;
     }
+    // second-contributor bits for the nonzero-pass kernel (dropped if some row cannot use them)
+    uint8_t *second = nullptr;
+    bool nz = false;
+    if (with_shared) {
+        int *d_bad = nullptr;
+        int bad = 1;
+        if (cudaMalloc(&second, (size_t)(ninc > 0 ? ninc : 1)) == cudaSuccess && cudaMalloc(&d_bad, 4) == cudaSuccess &&
+            cudaMemsetAsync(d_bad, 0, 4, s) == cudaSuccess) {
+            const unsigned g = (unsigned)((rp.ndof + 255) / 256);
+            if (rp.wide) k_second_masks<true><<<g, 256, 0, s>>>(rp, second, d_bad);
+            else k_second_masks<false><<<g, 256, 0, s>>>(rp, second, d_bad);
+            if (cudaMemcpyAsync(&bad, d_bad, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess)
+                bad = 1;
+        }
+        if (d_bad) cudaFree(d_bad);
+        nz = bad == 0;
+        if (!nz && second) {
+            cudaFree(second);
+            second = nullptr;
+        }
+        cudaGetLastError();
+    }
+    struct SecondGuard {
+        uint8_t *&p;
+        ~SecondGuard() {
+            if (p) cudaFree(p);
+        }
+    } second_guard{second};
     // Upload the blocks; for the shared-element lists, split any block whose distinct
     // elements exceed the kernel's capacity and rebuild (a few passes at most).
     for (int pass = 0;; pass++) {
@@ -712,11 +993,11 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
         if (block_inc == kSharedBlockInc)
             k_block_elems<kSharedBlockInc, kSharedMaxElems><<<out->nblocks, kSharedBlockInc, 0, s>>>(
                 rp, out->block_row, out->blk_nelem, out->blk_k0, out->blk_elem, out->inc_slot, out->inc_sorted,
-                nullptr);
+                second, nullptr);
         else
             k_block_elems<kBlockInc, kMaxBlockElems><<<out->nblocks, kBlockInc, 0, s>>>(
                 rp, out->block_row, out->blk_nelem, out->blk_k0, out->blk_elem, out->inc_slot, out->inc_sorted,
-                nullptr);
+                second, nullptr);
         std::vector<int32_t> nel((size_t)out->nblocks);
         if (cudaMemcpyAsync(nel.data(), out->blk_nelem, nel.size() * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) {
@@ -746,18 +1027,22 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
         for (int32_t b = 0; b < out->nblocks; b++) {
             next.push_back(starts[b]);
             const bool over = nel[b] > max_elems ||
-                              (!scnt.empty() && (scnt[2 * b] > kStageMaxNodes || scnt[2 * b + 1] > kStageMaxEdges));
+                              (!scnt.empty() && (scnt[2 * b] > kStageMaxNodes || scnt[2 * b + 1] > kStageMaxEdges)) ||
+                              (nz && rpp[starts[b + 1]] - rpp[starts[b]] > kNzMaxSpan);
             if (over && starts[b + 1] - starts[b] > 1) {
                 next.push_back(starts[b] + (starts[b + 1] - starts[b]) / 2);
                 split = true;
             } else if (nel[b] > max_elems) {
                 with_shared = false;  // one row alone exceeds the capacity
+            } else if (nz && rpp[starts[b + 1]] - rpp[starts[b]] > kNzMaxSpan) {
+                nz = false;  // one row alone exceeds the nonzero-pass capacity
             }
         }
         next.push_back(starts.back());
         if (!with_shared) break;
         if (!split) {
             out->shared_ok = 1;
+            out->nz_ok = nz ? 1 : 0;
             break;
         }
         if (pass >= 4) {
@@ -869,6 +1154,42 @@ int launch_rowblock_shared_jacobian(const RowBlockPlan &bp, const ElemData &m, c
     cudaError_t e = cudaPeekAtLastError();
     if (e != cudaSuccess) {
         set_error("shared row-block launch: %s", cudaGetErrorString(e));
+        return MAG_E_CUDA;
+    }
+    return MAG_OK;
+}
+
+}  // namespace mag
+
+namespace mag {
+
+int launch_rowblock_nz_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *sol,
+                                const QuadParams &qp, const MaterialParams &mp, int calcj, double *vals,
+                                double *res, cudaStream_t s) {
+    if (!bp.ok || !bp.shared_ok || !bp.nz_ok || !qp.standard_curl) return MAG_E_UNSUPPORTED;
+    RBArgs A{m, rp, sol, qp, mp, bp.block_row, vals, res};
+    const bool wide = rp.wide != 0, q4 = qp.nq == 4 && qp.uniform_w;
+    constexpr int BI = kSharedBlockInc, ME = kSharedMaxElems;
+    constexpr int sm = NzLayout<BI, ME>::bytes;
+#define MAG_NZ(CJ, Q, W)                                                                                 \
+    do {                                                                                                 \
+        auto kern = k_rowblock_nz<BI, ME, 4, CJ, Q, W>;                                                  \
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                     \
+        kern<<<bp.nblocks, BI, sm, s>>>(A, bp.blk_nelem, bp.blk_k0, bp.blk_elem, bp.inc_sorted);         \
+    } while (0)
+    if (calcj) {
+        if (q4) {
+            if (wide) MAG_NZ(true, true, true); else MAG_NZ(true, true, false);
+        } else {
+            if (wide) MAG_NZ(true, false, true); else MAG_NZ(true, false, false);
+        }
+    } else {
+        if (q4) MAG_NZ(false, true, false); else MAG_NZ(false, false, false);
+    }
+#undef MAG_NZ
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        set_error("nonzero-pass row-block launch: %s", cudaGetErrorString(e));
         return MAG_E_CUDA;
     }
     return MAG_OK;

@@ -13,7 +13,8 @@ constexpr int kBlockInc = 256;  // incidences per CTA == threads per CTA
 
 constexpr int kMaxBlockElems = 224;  // distinct elements per 256-incidence block the shared kernel holds
 constexpr int kSharedBlockInc = 256; // block size of the shared-element schedule (4 CTAs per SM)
-constexpr int kSharedMaxElems = 224; // distinct elements per block (larger blocks are split)
+constexpr int kSharedMaxElems = 192; // distinct elements per block (larger blocks are split)
+constexpr int kNzMaxSpan = 1024;     // CSR nonzeros per block of the nonzero-pass kernel (larger blocks are split)
 
 struct RowBlockPlan {
     int32_t *block_row = nullptr;  // [nblocks+1]
@@ -28,7 +29,11 @@ struct RowBlockPlan {
     int32_t *blk_elem = nullptr;   // [ninc] (first blk_nelem[b] entries after the block's offset)
     uint16_t *inc_slot = nullptr;  // [ninc] slot | local row << 8
     uint32_t *inc_sorted = nullptr; // [ninc] per block in element order: slot | local row << 8 | incidence << 16
+                                    // | second-contributor bits << 24 (when nz_ok)
     int shared_ok = 0;
+    // nonzero-pass kernel: every off-diagonal CSR entry has at most two contributions and
+    // inc_sorted carries, per incidence and local column, whether it is the second of them
+    int nz_ok = 0;
     // staging: per block its distinct nodes and edge dofs, and per distinct element a
     // record of local node / edge indices, tag and sign bits (exact offsets per block)
     int32_t *stg_cnt = nullptr;    // [nblocks][2] nodes, edges
@@ -53,5 +58,11 @@ int launch_rowblock_jacobian(const RowBlockPlan &bp, const ElemData &m, const Ro
 int launch_rowblock_shared_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp,
                                     const double *sol, const QuadParams &qp, const MaterialParams &mp, int calcj,
                                     double *vals, double *res, cudaStream_t s, bool staged = false);
+// Same result, bit for bit: shared-element blocks whose off-diagonal entries are placed
+// by the incidences themselves and stored by one pass over the block's nonzeros; only
+// the diagonal and the residual are summed per row (needs bp.nz_ok).
+int launch_rowblock_nz_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *sol,
+                                const QuadParams &qp, const MaterialParams &mp, int calcj, double *vals,
+                                double *res, cudaStream_t s);
 
 }  // namespace mag

@@ -351,8 +351,8 @@ def test_errors_are_reported(oracle_port):
 
 # ---- the three Jacobian schedules ------------------------------------------------------------
 
-SCHEDULES = (_lib.SCHEDULE_SHARED_ROW_BLOCKS, _lib.SCHEDULE_STAGED_ROW_BLOCKS, _lib.SCHEDULE_ROW_BLOCKS,
-             _lib.SCHEDULE_L2_RING, _lib.SCHEDULE_TWO_PASS)
+SCHEDULES = (_lib.SCHEDULE_SHARED_ROW_BLOCKS, _lib.SCHEDULE_NZ_ROW_BLOCKS, _lib.SCHEDULE_STAGED_ROW_BLOCKS,
+             _lib.SCHEDULE_ROW_BLOCKS, _lib.SCHEDULE_L2_RING, _lib.SCHEDULE_TWO_PASS)
 
 
 @pytest.mark.parametrize("n,seed", [(13, 21), (30, 22)])
@@ -363,7 +363,8 @@ def test_schedules_agree_bit_for_bit(oracle_port, n, seed):
     quadrature path."""
     mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, n, seed)
     plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
-    assert plan.info.schedule == _lib.SCHEDULE_SHARED_ROW_BLOCKS and plan.info.shared_staged == 0
+    assert plan.info.schedule == _lib.SCHEDULE_NZ_ROW_BLOCKS and plan.info.shared_staged == 0
+    assert plan.info.nz_pass == 1
     if n >= 30:
         assert 2 * plan.info.fused_ring_tiles < (mesh.num_elements + 255) // 256
     pk = material.pack_material_data(synth.standard_materials())
@@ -458,7 +459,7 @@ def test_wide_rows_match_oracle_on_every_schedule(oracle_port):
     I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, qw, curl, pk, True)
     ref = oracle_matrix(oracle_port, I, J, V, E, False)
     plan = AssemblyPlan(P, T, t2e, E, tags, sign)
-    assert plan.info.wide_positions == 1 and plan.info.max_row_nnz > 31
+    assert plan.info.wide_positions == 1 and plan.info.max_row_nnz > 31 and plan.info.nz_pass == 1
     plan.set_materials(pk)
     x = dev(sol)
     for sch in SCHEDULES:
@@ -470,3 +471,46 @@ def test_wide_rows_match_oracle_on_every_schedule(oracle_port):
     K = plan.stiffness(dev(np.full(T.shape[0], 800.0)))
     Ik, Jk, Vk = oracle_port.curl_curl(m, np.full(T.shape[0], 800.0), qw, curl)
     assert_csr_equal(plan.row_ptr, plan.col_idx, K, oracle_matrix(oracle_port, Ik, Jk, Vk, E, False))
+
+
+# ---- the nonzero-pass schedule's preconditions ----------------------------------------------
+
+def test_nz_schedule_rows_without_incidences_and_merged_dofs(oracle_port):
+    """Dofs that no element uses give empty CSR rows, which the nonzero pass skips; dofs shared
+    by two edges give off-diagonal entries with more than two contributions, which it cannot
+    place: the plan reports it unavailable and the default schedule stays exact."""
+    mesh = synth.kuhn_box(5, 4, 3, seed=4)
+    tags = synth.cube_layout(mesh)
+    edges, t2e, sign = oracle_port.generate_edges(mesh.T)
+    E = edges.shape[0]
+    pk = material.pack_material_data(synth.standard_materials())
+    qw, val, curl = quadrature.reference_data(2)
+    # (a) three unused dofs at the end
+    n = E + 3
+    m = mex_inputs(mesh.P, mesh.T, t2e, sign, tags)
+    sol = np.random.default_rng(5).normal(0, 0.05, n)
+    I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, qw, curl, pk, True)
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, n, tags, sign)
+    plan.set_materials(pk)
+    assert plan.info.nz_pass == 1
+    plan.set_schedule(_lib.SCHEDULE_NZ_ROW_BLOCKS)
+    v, r = plan.jacobian(dev(sol))
+    assert_csr_equal(plan.row_ptr, plan.col_idx, v, oracle_matrix(oracle_port, I, J, V, n, False))
+    assert bits_equal(host(r), oracle_port.sparse_vec(Ri, Rv, n))
+    # (b) two edges through the corner node that share no element, (0,1) and (0,6), carry
+    # one dof: entries coupling it with the diagonal edge from the corner get four
+    # contributions
+    assert list(edges[0]) == [0, 1] and list(edges[1]) == [0, 6]
+    assert not set(np.where(t2e == 0)[0]) & set(np.where(t2e == 1)[0])
+    dofs = np.where(t2e == 1, 0, t2e).astype(np.int32)
+    m2 = mex_inputs(mesh.P, mesh.T, dofs, sign, tags)
+    I, J, V, Ri, Rv = oracle_port.jacobian(m2, sol[:E], qw, curl, pk, True)
+    plan2 = AssemblyPlan(mesh.P, mesh.T, dofs, E, tags, sign)
+    plan2.set_materials(pk)
+    assert plan2.info.nz_pass == 0 and plan2.info.shared_blocks > 0
+    assert plan2.info.schedule == _lib.SCHEDULE_SHARED_ROW_BLOCKS
+    with pytest.raises(_lib.MagError):
+        plan2.set_schedule(_lib.SCHEDULE_NZ_ROW_BLOCKS)
+    v, r = plan2.jacobian(dev(sol[:E]))
+    assert_csr_equal(plan2.row_ptr, plan2.col_idx, v, oracle_matrix(oracle_port, I, J, V, E, False))
+    assert bits_equal(host(r), oracle_port.sparse_vec(Ri, Rv, E))
