@@ -44,25 +44,44 @@ class AFT:
     def num_harmonics(self):
         return self.harmonics.size
 
+    def device_operators(self):
+        """D and P split into real / imaginary float64 CUDA tensors in the library's layout
+        (D as [K][N], P as [N][K]); made once and kept."""
+        if getattr(self, "_dev", None) is None:
+            dev = torch.device("cuda")
+
+            def t(a):
+                return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+
+            self._dev = (t(np.real(self.D).T), t(np.imag(self.D).T), t(np.real(self.P).T), t(np.imag(self.P).T))
+        return self._dev
+
 
 def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
 
 
 def assemble_hbfem(plan, sol, aft: AFT, calc_j: bool = True, stream=None):
-    """Harmonic residual and DC Jacobian block for the harmonic field sol [Ndof, K] (complex).
+    """Harmonic residual and DC Jacobian block for the harmonic field sol [Ndof, K] (complex):
+    a host array, or a CUDA tensor (complex128 [Ndof, K], or a (re, im) pair of float64
+    [K, Ndof] tensors in the library's layout, which is used as is).
 
     Returns (R complex [K, Ndof] on the GPU, vals [nnz] float64 or None)."""
     L = _lib.lib()
     K, N = aft.num_harmonics, aft.num_time_steps
     dev = torch.device("cuda")
-    sol = np.asarray(sol)
-    sr = torch.as_tensor(np.ascontiguousarray(np.real(sol).T), dtype=torch.float64, device=dev)  # [K][Ndof]
-    si = torch.as_tensor(np.ascontiguousarray(np.imag(sol).T), dtype=torch.float64, device=dev)
-    dr = torch.as_tensor(np.ascontiguousarray(np.real(aft.D).T), dtype=torch.float64, device=dev)  # [K][N]
-    di = torch.as_tensor(np.ascontiguousarray(np.imag(aft.D).T), dtype=torch.float64, device=dev)
-    pr = torch.as_tensor(np.ascontiguousarray(np.real(aft.P).T), dtype=torch.float64, device=dev)  # [N][K]
-    pi = torch.as_tensor(np.ascontiguousarray(np.imag(aft.P).T), dtype=torch.float64, device=dev)
+    if isinstance(sol, tuple):
+        sr, si = sol
+    elif isinstance(sol, torch.Tensor):
+        sr = torch.real(sol).T.contiguous().to(torch.float64)  # [K][Ndof]
+        si = torch.imag(sol).T.contiguous().to(torch.float64) if sol.is_complex() else None
+    else:
+        sol = np.asarray(sol)
+        sr = torch.as_tensor(np.ascontiguousarray(np.real(sol).T), dtype=torch.float64, device=dev)  # [K][Ndof]
+        si = torch.as_tensor(np.ascontiguousarray(np.imag(sol).T), dtype=torch.float64, device=dev)
+    if sr.shape != (K, plan.num_dofs) or not sr.is_cuda or (si is not None and si.shape != sr.shape):
+        raise ValueError("harmonic field must be [Ndof, K] for the AFT's K harmonics")
+    dr, di, pr, pi = aft.device_operators()
     rre = torch.empty((K, plan.num_dofs), dtype=torch.float64, device=dev)
     rim = torch.empty_like(rre)
     vals = plan.new_values() if calc_j else None

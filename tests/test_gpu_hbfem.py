@@ -63,3 +63,19 @@ def test_hbfem_residual_only_and_errors(oracle_port):
     from magpackage_b200 import _lib
     with pytest.raises(_lib.MagError):
         assemble_hbfem(plan, np.zeros((E, 17)), AFT(list(range(17))), False)  # more than 16 harmonics
+
+
+def test_hbfem_device_resident_field_gives_the_same_bits(oracle_port):
+    """A complex CUDA tensor or a (re, im) pair already in [K, Ndof] layout is used without
+    a host round trip and gives the host array's result."""
+    plan, m, pk, sol, E = _case(oracle_port, (0, 1, 3))
+    aft = AFT((0, 1, 3))
+    R0, v0 = assemble_hbfem(plan, sol, aft, True)
+    R1, v1 = assemble_hbfem(plan, torch.as_tensor(sol, device="cuda"), aft, True)
+    pair = (torch.as_tensor(np.ascontiguousarray(sol.real.T), device="cuda"),
+            torch.as_tensor(np.ascontiguousarray(sol.imag.T), device="cuda"))
+    R2, v2 = assemble_hbfem(plan, pair, aft, True)
+    for R, v in ((R1, v1), (R2, v2)):
+        assert torch.equal(R, R0) and torch.equal(v, v0)
+    with pytest.raises(ValueError):
+        assemble_hbfem(plan, pair[0][:2], aft, False)
