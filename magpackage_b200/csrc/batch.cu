@@ -33,6 +33,12 @@ struct BatchItem {
     int32_t block;
 };
 
+// Nonzeros of a block the slot path holds: four slot arrays (K and M, two slots per
+// nonzero) plus per-incidence diagonals and row offsets fit in the 24 * BI doubles of the
+// row-phase buffers. A block's span is at most 6 * BI; larger spans take the row phase.
+template <int BI>
+constexpr int kSlotSpan = 5 * BI;
+
 template <int BI>
 __device__ void complex_block(const BatchInstance &I, int blk, double *sk, double *sm, double *acc_k,
                               double *acc_m, int *s_rp, int *s_ip, const double *sval) {
@@ -46,6 +52,20 @@ __device__ void complex_block(const BatchInstance &I, int blk, double *sk, doubl
     __syncthreads();
     const int k0 = s_ip[0], ninc = s_ip[nrows] - k0;
     const int base = s_rp[0], span = s_rp[nrows] - base;
+    // slot path: each off-diagonal entry of K and M has at most two contributions (the
+    // tetrahedra sharing a face) and (0 + a) + b does not depend on their order, so the
+    // incidences place them directly; only the diagonals are summed per row
+    const bool slots = I.second != nullptr && span <= kSlotSpan<BI>;
+    double *slot_k = sk, *slot_m = sk + 2 * kSlotSpan<BI>;  // [span][2] each
+    double *sdiag = sk + 4 * kSlotSpan<BI>;                   // [ninc][2]: K, M diagonal entries
+    uint16_t *sroff = reinterpret_cast<uint16_t *>(sdiag + 2 * BI);  // [ninc]: row's first nonzero
+    static_assert(4 * kSlotSpan<BI> + 2 * BI + BI / 4 <= 24 * BI, "slot path fits the row-phase buffers");
+    if (slots) {
+        for (int r = tid; r < nrows; r += BI)
+            for (int k = s_ip[r]; k < s_ip[r + 1]; k++) sroff[k - k0] = (uint16_t)(s_rp[r] - base);
+        for (int i = tid; i < 4 * span; i += BI) (i < 2 * span ? slot_k[i] : slot_m[i - 2 * span]) = 0.0;
+        __syncthreads();
+    }
     if (tid < ninc) {
         uint32_t ew = __ldg(I.rp.inc_elem + k0 + tid);
         const int64_t e = ew & 0x1FFFFFFFu;
@@ -68,17 +88,16 @@ __device__ void complex_block(const BatchInstance &I, int blk, double *sk, doubl
         }
         const double nu = I.nu[e];
         const double w0 = I.qw[0] * g.adet;
-        double *ok = sk + tid * 6;
+        double krow[6];
 #pragma unroll
         for (int j = 0; j < 6; j++) {
             double u = (dot3(Cl, C[j]) * nu) * w0;
             double kv = I.nq4 ? ((u + u) + u) + u : u;
             if (!I.nq4)
                 for (int q = 1; q < I.nq; q++) kv = kv + (dot3(Cl, C[j]) * nu) * (I.qw[q] * g.adet);
-            ok[j] = flip(kv, si ^ ((sb >> j) & 1));
+            krow[j] = flip(kv, si ^ ((sb >> j) & 1));
         }
         // sigma-mass row: sum_q (N_loc . N_j * sigma) * w_q, N = J^{-T} N_ref
-        double *om = sm + tid * 6;
         const double sigma = I.sigma ? I.sigma[e] : 1.0;
         double mrow[6] = {0, 0, 0, 0, 0, 0};
         if (fabs(sigma) > 1e-12) {
@@ -106,7 +125,72 @@ __device__ void complex_block(const BatchInstance &I, int blk, double *sk, doubl
             }
         }
 #pragma unroll
-        for (int j = 0; j < 6; j++) om[j] = flip(mrow[j], si ^ ((sb >> j) & 1));
+        for (int j = 0; j < 6; j++) mrow[j] = flip(mrow[j], si ^ ((sb >> j) & 1));
+        if (slots) {
+            unsigned p[6];
+            if (!I.rp.wide) {
+                const uint32_t pw = __ldg(I.rp.inc_pos + k0 + tid);
+#pragma unroll
+                for (int j = 0; j < 6; j++) p[j] = (pw >> (5 * j)) & 31u;
+            } else {
+                const uint32_t w0p = __ldg(I.rp.inc_pos + 2 * (int64_t)(k0 + tid));
+                const uint32_t w1p = __ldg(I.rp.inc_pos + 2 * (int64_t)(k0 + tid) + 1);
+#pragma unroll
+                for (int j = 0; j < 6; j++) p[j] = (j < 4 ? (w0p >> (8 * j)) : (w1p >> (8 * (j - 4)))) & 255u;
+            }
+            const unsigned none = I.rp.wide ? (unsigned)kWideMaxRow : (unsigned)kCompactMaxRow;
+            const unsigned second = __ldg(I.second + k0 + tid);
+            const int off = sroff[tid];
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                if (j == loc) {
+                    sdiag[2 * tid] = krow[j];
+                    sdiag[2 * tid + 1] = mrow[j];
+                } else if (p[j] != none) {
+                    const int at = 2 * (off + (int)p[j]) + (int)((second >> j) & 1);
+                    slot_k[at] = krow[j];
+                    slot_m[at] = mrow[j];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                sk[tid * 6 + j] = krow[j];
+                sm[tid * 6 + j] = mrow[j];
+            }
+        }
+    }
+    double2 *out = reinterpret_cast<double2 *>(I.vals);
+    if (slots) {
+        __syncthreads();
+        // diagonals: one thread per row, its incidences in ascending element order
+        for (int r = tid; r < nrows; r += BI) {
+            const int i0 = s_ip[r] - k0, i1 = s_ip[r + 1] - k0;
+            if (i1 <= i0) continue;
+            double dk = 0.0, dm = 0.0;
+            for (int k = i0; k < i1; k++) {
+                dk = dk + sdiag[2 * k];
+                dm = dm + sdiag[2 * k + 1];
+            }
+            const int kf = k0 + i0;
+            const int l = (int)(__ldg(I.rp.inc_elem + kf) >> 29);
+            unsigned pd;
+            if (!I.rp.wide) {
+                pd = (__ldg(I.rp.inc_pos + kf) >> (5 * l)) & 31u;
+            } else {
+                pd = (l < 4 ? (__ldg(I.rp.inc_pos + 2 * (int64_t)kf) >> (8 * l))
+                            : (__ldg(I.rp.inc_pos + 2 * (int64_t)kf + 1) >> (8 * (l - 4)))) & 255u;
+            }
+            const int at = 2 * (s_rp[r] - base + (int)pd);
+            slot_k[at] = dk;
+            slot_m[at] = dm;
+        }
+        __syncthreads();
+        for (int i = tid; i < span; i += BI)
+            out[base + i] = make_double2((0.0 + slot_k[2 * i]) + slot_k[2 * i + 1],
+                                         I.omega * ((0.0 + slot_m[2 * i]) + slot_m[2 * i + 1]));
+        __syncthreads();
+        return;
     }
     for (int i = tid; i < span; i += BI) {
         acc_k[i] = 0.0;
@@ -141,7 +225,6 @@ __device__ void complex_block(const BatchInstance &I, int blk, double *sk, doubl
         }
     }
     __syncthreads();
-    double2 *out = reinterpret_cast<double2 *>(I.vals);
     for (int i = tid; i < span; i += BI) out[base + i] = make_double2(acc_k[i], I.omega * acc_m[i]);
     __syncthreads();
 }

@@ -17,6 +17,7 @@ struct BatchInstance {
     const double *nu;          // [Ne]
     const double *sigma;       // [Ne] or NULL (sigma = 1)
     const double *val_ref;     // [18 * nq] reference basis values
+    const uint8_t *second;     // per incidence: second-contributor bits, or NULL (row phase only)
     double qw[kMaxQuad];
     int nq;
     int nq4;                   // 4 equal weights

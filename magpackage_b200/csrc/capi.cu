@@ -307,7 +307,8 @@ struct mag_mesh {
     int has_mat = 0;
     FusedPlan fused;
     RowBlockPlan rowblock;
-    RowBlockPlan rowshared;  // 128-incidence blocks with per-block distinct-element lists
+    RowBlockPlan rowshared;  // 256-incidence blocks with per-block distinct-element lists
+    uint8_t *second = nullptr;  // per incidence: second-contributor bits (NULL: some row has > 2)
     int schedule = MAG_SCHEDULE_ROW_BLOCKS;
     int64_t bytes = 0;
 
@@ -321,7 +322,7 @@ namespace {
 
 void destroy_mesh(mag_mesh *m) {
     if (!m) return;
-    void *ptrs[] = {m->xyz, m->tet, m->dofs, m->tags, m->signbits, m->scratch, m->d_ref, m->mat.mem};
+    void *ptrs[] = {m->xyz, m->tet, m->dofs, m->tags, m->signbits, m->scratch, m->d_ref, m->mat.mem, m->second};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     free_pattern(&m->pat, nullptr);
@@ -459,7 +460,8 @@ int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t N
         free_rowblock_plan(&m->rowblock);
         cudaGetLastError();
     }
-    if (build_rowblock_plan(m->rows(), &m->rowshared, s, kSharedBlockInc, true) == MAG_OK &&
+    if (build_second_masks(m->rows(), m->pat.ninc, &m->second, s) == MAG_OK && m->second) m->bytes += m->pat.ninc;
+    if (build_rowblock_plan(m->rows(), &m->rowshared, s, kSharedBlockInc, true, nullptr, m->second) == MAG_OK &&
         m->rowshared.shared_ok) {
         m->bytes += m->rowshared.bytes;
     } else {
@@ -732,7 +734,7 @@ int mag_mesh_set_option(mag_mesh *m, int option, int64_t value) {
             // the staging tables are built on first request (blocks re-split to their capacity)
             RowBlockPlan staged{};
             const ElemData ed = m->elems();
-            if (build_rowblock_plan(m->rows(), &staged, nullptr, kSharedBlockInc, true, &ed) == MAG_OK &&
+            if (build_rowblock_plan(m->rows(), &staged, nullptr, kSharedBlockInc, true, &ed, m->second) == MAG_OK &&
                 staged.shared_ok && staged.staged_ok) {
                 m->bytes += staged.bytes - m->rowshared.bytes;
                 free_rowblock_plan(&m->rowshared);
@@ -860,6 +862,7 @@ int mag_batch_create(mag_mesh *const *meshes, int n, const double *const *d_nu, 
         bi.nu = d_nu[i];
         bi.sigma = d_sigma ? d_sigma[i] : nullptr;
         bi.val_ref = m->qp.val_ref;
+        bi.second = m->second;
         bi.nq = m->qp.nq;
         for (int q = 0; q < m->qp.nq; q++) bi.qw[q] = m->qp.qw[q];
         bi.nq4 = (m->qp.nq == 4 && m->qp.uniform_w) ? 1 : 0;

@@ -911,8 +911,32 @@ void build_stage(const ElemData &m, RowBlockPlan *out, cudaStream_t s) {
 
 }  // namespace
 
+int build_second_masks(const RowPlan &rp, int64_t ninc, uint8_t **out, cudaStream_t s) {
+    *out = nullptr;
+    uint8_t *second = nullptr;
+    int *d_bad = nullptr;
+    int bad = 1;
+    if (cudaMalloc(&second, (size_t)(ninc > 0 ? ninc : 1)) == cudaSuccess && cudaMalloc(&d_bad, 4) == cudaSuccess &&
+        cudaMemsetAsync(d_bad, 0, 4, s) == cudaSuccess) {
+        const unsigned g = (unsigned)((rp.ndof + 255) / 256);
+        if (rp.wide) k_second_masks<true><<<g, 256, 0, s>>>(rp, second, d_bad);
+        else k_second_masks<false><<<g, 256, 0, s>>>(rp, second, d_bad);
+        if (cudaMemcpyAsync(&bad, d_bad, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            bad = 1;
+    }
+    if (d_bad) cudaFree(d_bad);
+    cudaGetLastError();
+    if (bad) {
+        if (second) cudaFree(second);
+        return MAG_OK;  // no masks: the nonzero-pass kernels are not available for this mesh
+    }
+    *out = second;
+    return MAG_OK;
+}
+
 int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc, bool with_shared,
-                        const ElemData *stage_mesh) {
+                        const ElemData *stage_mesh, const uint8_t *second) {
     *out = RowBlockPlan{};
     std::vector<int32_t> ip((size_t)rp.ndof + 1), rpp((size_t)rp.ndof + 1);
     MAG_CUDA_TRY(cudaMemcpyAsync(ip.data(), rp.inc_ptr, ip.size() * 4, cudaMemcpyDeviceToHost, s));
@@ -943,35 +967,8 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
             cudaMalloc(&out->inc_sorted, (size_t)(ninc > 0 ? ninc : 1) * 4) != cudaSuccess)
             with_shared = false;
     }
-    // second-contributor bits for the nonzero-pass kernel (dropped if some row cannot use them)
-    uint8_t *second = nullptr;
-    bool nz = false;
-    if (with_shared) {
-        int *d_bad = nullptr;
-        int bad = 1;
-        if (cudaMalloc(&second, (size_t)(ninc > 0 ? ninc : 1)) == cudaSuccess && cudaMalloc(&d_bad, 4) == cudaSuccess &&
-            cudaMemsetAsync(d_bad, 0, 4, s) == cudaSuccess) {
-            const unsigned g = (unsigned)((rp.ndof + 255) / 256);
-            if (rp.wide) k_second_masks<true><<<g, 256, 0, s>>>(rp, second, d_bad);
-            else k_second_masks<false><<<g, 256, 0, s>>>(rp, second, d_bad);
-            if (cudaMemcpyAsync(&bad, d_bad, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-                cudaStreamSynchronize(s) != cudaSuccess)
-                bad = 1;
-        }
-        if (d_bad) cudaFree(d_bad);
-        nz = bad == 0;
-        if (!nz && second) {
-            cudaFree(second);
-            second = nullptr;
-        }
-        cudaGetLastError();
-    }
-    struct SecondGuard {
-        uint8_t *&p;
-        ~SecondGuard() {
-            if (p) cudaFree(p);
-        }
-    } second_guard{second};
+    // second-contributor bits (mesh-owned, built by build_second_masks) enable the nonzero-pass kernel
+    bool nz = with_shared && second != nullptr;
     // Upload the blocks; for the shared-element lists, split any block whose distinct
     // elements exceed the kernel's capacity and rebuild (a few passes at most).
     for (int pass = 0;; pass++) {

@@ -47,8 +47,15 @@ struct RowBlockPlan {
 constexpr int kStageMaxNodes = 192;  // distinct nodes per block the staged kernel holds
 constexpr int kStageMaxEdges = 512;  // distinct edge dofs per block
 
+// Per incidence (row order) bit j: the incidence is the second of the (at most two)
+// contributions to its column j's off-diagonal entry. *out = NULL when some row breaks
+// that bound (a repeated dof): the nonzero-pass kernels are then unavailable. The
+// caller owns and frees the array (ninc bytes).
+int build_second_masks(const RowPlan &rp, int64_t ninc, uint8_t **out, cudaStream_t s);
+// `second`: the masks above, or NULL (no nonzero-pass plan).
 int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc = kBlockInc,
-                        bool with_shared = false, const ElemData *stage_mesh = nullptr);
+                        bool with_shared = false, const ElemData *stage_mesh = nullptr,
+                        const uint8_t *second = nullptr);
 void free_rowblock_plan(RowBlockPlan *p);
 int launch_rowblock_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *sol,
                              const QuadParams &qp, const MaterialParams &mp, int calcj, double *vals,

@@ -430,6 +430,45 @@ def test_batched_complex_matches_oracle(oracle_port):
     batch.close()
 
 
+def test_batched_complex_slot_and_row_paths(oracle_port):
+    """A batch mixing a mesh whose off-diagonal entries have at most two contributions (slot
+    path) with one where a dof shared by two edges breaks that bound (row phase) is exact on
+    every variant."""
+    from magpackage_b200.plan import ComplexBatch
+
+    qw, val, curl = quadrature.reference_data(2)
+    plans, nus, sigmas, refs, omegas = [], [], [], [], []
+    for merged in (False, True):
+        mesh = synth.kuhn_box(5, 4, 3, seed=4)
+        tags = synth.cube_layout(mesh)
+        edges, t2e, sign = oracle_port.generate_edges(mesh.T)
+        E = edges.shape[0]
+        dofs = np.where(t2e == 1, 0, t2e).astype(np.int32) if merged else t2e
+        m = mex_inputs(mesh.P, mesh.T, dofs, sign, tags)
+        rng = np.random.default_rng(7 + merged)
+        nu = rng.uniform(0.5, 2.0, mesh.num_elements) * material.NU0
+        sigma = np.where(tags == synth.ALUMINIUM, synth.SIGMA_AL, 0.0)
+        plan = AssemblyPlan(mesh.P, mesh.T, dofs, E, tags, sign)
+        assert plan.info.nz_pass == (0 if merged else 1)
+        I, J, Vk = oracle_port.curl_curl(m, nu, qw, curl)
+        _, _, Vm = oracle_port.mass(m, sigma, qw, val)
+        plans.append(plan)
+        nus.append(dev(nu))
+        sigmas.append(dev(sigma))
+        omegas.append(2 * np.pi * (50.0 + 25.0 * merged))
+        refs.append((oracle_matrix(oracle_port, I, J, Vk, E, False), oracle_matrix(oracle_port, I, J, Vm, E, False)))
+    batch = ComplexBatch(plans, nus, sigmas, omegas)
+    _, times, _ = batch.tuning()
+    for variant in range(len(times)):
+        batch.select(variant)
+        vals = batch.assemble()
+        torch.cuda.synchronize()
+        for plan, v, (kref, mref), omega in zip(plans, vals, refs, omegas):
+            assert_csr_equal(plan.row_ptr, plan.col_idx, v.real.contiguous(), kref)
+            assert bits_equal(host(v.imag.contiguous()), omega * mref[2]), variant
+    batch.close()
+
+
 # ---- wide rows ---------------------------------------------------------------------------
 
 def _pinwheel(n_blades=12, seed=0):
