@@ -432,30 +432,36 @@ def test_batched_complex_matches_oracle(oracle_port):
 
 def test_batched_complex_slot_and_row_paths(oracle_port):
     """A batch mixing a mesh whose off-diagonal entries have at most two contributions (slot
-    path) with one where a dof shared by two edges breaks that bound (row phase) is exact on
-    every variant."""
+    path), one where a dof shared by two edges breaks that bound (row phase) and one with
+    rows of more than 31 entries (slot path, wide positions) is exact on every variant."""
     from magpackage_b200.plan import ComplexBatch
 
     qw, val, curl = quadrature.reference_data(2)
     plans, nus, sigmas, refs, omegas = [], [], [], [], []
-    for merged in (False, True):
-        mesh = synth.kuhn_box(5, 4, 3, seed=4)
-        tags = synth.cube_layout(mesh)
-        edges, t2e, sign = oracle_port.generate_edges(mesh.T)
+    for kind in ("box", "merged", "pinwheel"):
+        if kind == "pinwheel":
+            P, T = _pinwheel()
+            tags = np.where(np.arange(T.shape[0]) % 3 == 0, synth.ALUMINIUM, synth.AIR).astype(np.int32)
+        else:
+            mesh = synth.kuhn_box(5, 4, 3, seed=4)
+            P, T, tags = mesh.P, mesh.T, synth.cube_layout(mesh)
+        edges, t2e, sign = oracle_port.generate_edges(T)
         E = edges.shape[0]
+        merged = kind == "merged"
         dofs = np.where(t2e == 1, 0, t2e).astype(np.int32) if merged else t2e
-        m = mex_inputs(mesh.P, mesh.T, dofs, sign, tags)
-        rng = np.random.default_rng(7 + merged)
-        nu = rng.uniform(0.5, 2.0, mesh.num_elements) * material.NU0
+        m = mex_inputs(P, T, dofs, sign, tags)
+        rng = np.random.default_rng(7 + len(plans))
+        nu = rng.uniform(0.5, 2.0, T.shape[0]) * material.NU0
         sigma = np.where(tags == synth.ALUMINIUM, synth.SIGMA_AL, 0.0)
-        plan = AssemblyPlan(mesh.P, mesh.T, dofs, E, tags, sign)
+        plan = AssemblyPlan(P, T, dofs, E, tags, sign)
         assert plan.info.nz_pass == (0 if merged else 1)
+        assert plan.info.wide_positions == (1 if kind == "pinwheel" else 0)
         I, J, Vk = oracle_port.curl_curl(m, nu, qw, curl)
         _, _, Vm = oracle_port.mass(m, sigma, qw, val)
         plans.append(plan)
         nus.append(dev(nu))
         sigmas.append(dev(sigma))
-        omegas.append(2 * np.pi * (50.0 + 25.0 * merged))
+        omegas.append(2 * np.pi * (50.0 + 25.0 * len(plans)))
         refs.append((oracle_matrix(oracle_port, I, J, Vk, E, False), oracle_matrix(oracle_port, I, J, Vm, E, False)))
     batch = ComplexBatch(plans, nus, sigmas, omegas)
     _, times, _ = batch.tuning()
