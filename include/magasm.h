@@ -141,7 +141,9 @@ int mag_assemble_jacobian(mag_mesh *mesh, const double *d_sol, double *d_vals, d
                           int calc_j, void *stream);
 
 /* Curl-curl stiffness K(nu) with a per-element reluctivity d_nu [Ne]
- * (assemble_curl_curl_kernel_mex.cpp:18-121 + Assembler.m:37-38). */
+ * (assemble_curl_curl_kernel_mex.cpp:18-121 + Assembler.m:37-38). Under
+ * MAG_SCHEDULE_NZ_ROW_BLOCKS (the default when available) one launch without the element
+ * scratch; under the other schedules the element kernel and the row reduction. Same bits. */
 int mag_assemble_stiffness(mag_mesh *mesh, const double *d_nu, double *d_vals, void *stream);
 
 /* Harmonic-balance assembly (assemble_hbfem_kernel_mex.cpp:26-258, called through

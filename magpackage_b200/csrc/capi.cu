@@ -592,6 +592,10 @@ int mag_assemble_stiffness(mag_mesh *m, const double *d_nu, double *d_vals, void
         return MAG_E_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
+    if (m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS && m->rowshared.nz_ok && m->qp.standard_curl) {
+        MAG_TRY(launch_rowblock_nz_stiffness(m->rowshared, m->elems(), m->rows(), d_nu, m->qp, d_vals, s));
+        return finish(s);
+    }
     MAG_TRY(launch_stiffness_elems(m->elems(), d_nu, m->qp, m->scratch, s));
     MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, d_vals, nullptr, s));
     return finish(s);

@@ -66,6 +66,7 @@ struct RBArgs {
     const int32_t *block_row;  // [nblocks+1] first row of each block
     double *vals;
     double *res;
+    const double *nu_e;        // [Ne] per-element reluctivity (stiffness mode of k_rowblock_nz)
 };
 
 constexpr int kSv = 9;  // shared-memory stride (doubles) of one incidence's values
@@ -680,7 +681,11 @@ struct NzLayout {
 // its diagonal entry and residual into per-incidence slots. B1: one thread per row sums
 // the diagonal and the residual over its incidences in ascending element order. B2: one
 // thread per nonzero stores (0 + slot 0) + slot 1, coalesced. Same bits as k_rowblock.
-template <int BI, int MAXE, int MINB, bool CALCJ, bool Q4, bool WIDE>
+//
+// STIFF: the curl-curl matrix K(nu) with the per-element reluctivity A.nu_e instead
+// (assemble_curl_curl_kernel_mex.cpp:94-101: (C_i . C_j) nu w summed over the points, the
+// Jacobian's entry with d nu = 0, same operation order); no solution, no residual.
+template <int BI, int MAXE, int MINB, bool CALCJ, bool Q4, bool WIDE, bool STIFF = false>
 __global__ void __launch_bounds__(BI, MINB) k_rowblock_nz(RBArgs A, const int32_t *__restrict__ blk_nelem,
                                                           const int32_t *__restrict__ blk_k0,
                                                           const int32_t *__restrict__ blk_elem,
@@ -727,41 +732,61 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_nz(RBArgs A, const int32_
         for (int i = tid; i < span; i += BI) nzv[i] = make_double2(0.0, 0.0);
     // phase A1: one thread per distinct element (the plan keeps nel <= MAXE)
     if (tid < nel && tid < MAXE) {
-        const int64_t e = blk_elem[k0 + tid];
-        const int4 tt = A.m.tet[e];
-        int d[6];
-        load_dofs(A.m.dofs, e, d);
-        const unsigned sb = A.m.signbits ? A.m.signbits[e] : derived_signs(tt);
-        const int tag = A.m.tags[e];
-        Geo g;
-        geometry(A.m.xyz, tt, g);
-        double a[6];
+        if (STIFF) {
+            const int64_t e = blk_elem[k0 + tid];
+            const int4 tt = A.m.tet[e];
+            const unsigned sb = A.m.signbits ? A.m.signbits[e] : derived_signs(tt);
+            Geo g;
+            geometry(A.m.xyz, tt, g);
+            ElemRec &R = rec[tid];
 #pragma unroll
-        for (int i = 0; i < 6; i++) a[i] = d[i] >= 0 ? flip(__ldg(A.sol + d[i]), (sb >> i) & 1) : 0.0;
-        double C[6][3];
-        curls_standard(g, C);
-        double B[3];
+            for (int r = 0; r < 3; r++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            double v = a[0] * C[0][c];
+                for (int c = 0; c < 3; c++) R.J[3 * r + c] = g.J[r][c];
+            R.r2 = 2.0 * g.rdet;
 #pragma unroll
-            for (int i = 1; i < 6; i++) v = v + a[i] * C[i][c];
-            B[c] = v;
+            for (int j = 0; j < 6; j++) R.b[j] = 0.0;
+            R.nu = __ldg(A.nu_e + e);
+            R.g2 = 0.0;
+            R.adet = g.adet;
+            rsb[tid] = sb;
+        } else {
+            const int64_t e = blk_elem[k0 + tid];
+            const int4 tt = A.m.tet[e];
+            int d[6];
+            load_dofs(A.m.dofs, e, d);
+            const unsigned sb = A.m.signbits ? A.m.signbits[e] : derived_signs(tt);
+            const int tag = A.m.tags[e];
+            Geo g;
+            geometry(A.m.xyz, tt, g);
+            double a[6];
+#pragma unroll
+            for (int i = 0; i < 6; i++) a[i] = d[i] >= 0 ? flip(__ldg(A.sol + d[i]), (sb >> i) & 1) : 0.0;
+            double C[6][3];
+            curls_standard(g, C);
+            double B[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                double v = a[0] * C[0][c];
+#pragma unroll
+                for (int i = 1; i < 6; i++) v = v + a[i] * C[i][c];
+                B[c] = v;
+            }
+            double nu, dnu;
+            material_eval(A.mp, tag, dot3(B, B), nu, dnu);
+            ElemRec &R = rec[tid];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) R.J[3 * r + c] = g.J[r][c];
+            R.r2 = 2.0 * g.rdet;
+#pragma unroll
+            for (int j = 0; j < 6; j++) R.b[j] = dot3(B, C[j]);
+            R.nu = nu;
+            R.g2 = 2.0 * dnu;
+            R.adet = g.adet;
+            rsb[tid] = sb;
         }
-        double nu, dnu;
-        material_eval(A.mp, tag, dot3(B, B), nu, dnu);
-        ElemRec &R = rec[tid];
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) R.J[3 * r + c] = g.J[r][c];
-        R.r2 = 2.0 * g.rdet;
-#pragma unroll
-        for (int j = 0; j < 6; j++) R.b[j] = dot3(B, C[j]);
-        R.nu = nu;
-        R.g2 = 2.0 * dnu;
-        R.adet = g.adet;
-        rsb[tid] = sb;
     }
     __syncthreads();
     // phase A2: one thread per incidence, walking them in element order
@@ -831,7 +856,7 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_nz(RBArgs A, const int32_
             racc = racc + v.x;
             if (CALCJ) dacc = dacc + v.y;
         }
-        A.res[a0 + r] = racc;
+        if (!STIFF) A.res[a0 + r] = racc;
         if (CALCJ && i1 > i0) {
             const int l = sloc[i0];
             unsigned pd;
@@ -1187,6 +1212,37 @@ int launch_rowblock_nz_jacobian(const RowBlockPlan &bp, const ElemData &m, const
     cudaError_t e = cudaPeekAtLastError();
     if (e != cudaSuccess) {
         set_error("nonzero-pass row-block launch: %s", cudaGetErrorString(e));
+        return MAG_E_CUDA;
+    }
+    return MAG_OK;
+}
+
+}  // namespace mag
+
+namespace mag {
+
+int launch_rowblock_nz_stiffness(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *nu,
+                                 const QuadParams &qp, double *vals, cudaStream_t s) {
+    if (!bp.ok || !bp.shared_ok || !bp.nz_ok || !qp.standard_curl || !nu || !vals) return MAG_E_UNSUPPORTED;
+    RBArgs A{m, rp, nullptr, qp, MaterialParams{}, bp.block_row, vals, nullptr, nu};
+    const bool wide = rp.wide != 0, q4 = qp.nq == 4 && qp.uniform_w;
+    constexpr int BI = kSharedBlockInc, ME = kSharedMaxElems;
+    constexpr int sm = NzLayout<BI, ME>::bytes;
+#define MAG_NZK(Q, W)                                                                                    \
+    do {                                                                                                 \
+        auto kern = k_rowblock_nz<BI, ME, 4, true, Q, W, true>;                                          \
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                     \
+        kern<<<bp.nblocks, BI, sm, s>>>(A, bp.blk_nelem, bp.blk_k0, bp.blk_elem, bp.inc_sorted);         \
+    } while (0)
+    if (q4) {
+        if (wide) MAG_NZK(true, true); else MAG_NZK(true, false);
+    } else {
+        if (wide) MAG_NZK(false, true); else MAG_NZK(false, false);
+    }
+#undef MAG_NZK
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        set_error("nonzero-pass stiffness launch: %s", cudaGetErrorString(e));
         return MAG_E_CUDA;
     }
     return MAG_OK;

@@ -71,5 +71,9 @@ int launch_rowblock_shared_jacobian(const RowBlockPlan &bp, const ElemData &m, c
 int launch_rowblock_nz_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *sol,
                                 const QuadParams &qp, const MaterialParams &mp, int calcj, double *vals,
                                 double *res, cudaStream_t s);
+// The curl-curl matrix K(nu) (per-element reluctivity nu [Ne]) with the same kernel: bit for
+// bit the two-pass stiffness assembly, one launch, no scratch (needs bp.nz_ok).
+int launch_rowblock_nz_stiffness(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *nu,
+                                 const QuadParams &qp, double *vals, cudaStream_t s);
 
 }  // namespace mag

@@ -559,3 +559,31 @@ def test_nz_schedule_rows_without_incidences_and_merged_dofs(oracle_port):
     v, r = plan2.jacobian(dev(sol[:E]))
     assert_csr_equal(plan2.row_ptr, plan2.col_idx, v, oracle_matrix(oracle_port, I, J, V, E, False))
     assert bits_equal(host(r), oracle_port.sparse_vec(Ri, Rv, E))
+
+
+def test_stiffness_nonzero_pass_matches_oracle(oracle_port):
+    """K(nu) under the nonzero-pass schedule (one launch, no scratch) equals the oracle's
+    curl-curl sparse() and the two-pass assembly, on the standard and a general quadrature,
+    on a box and on a mesh with rows of more than 31 entries."""
+    qw, val, curl = quadrature.reference_data(2)
+    qw2 = np.array([0.05, 0.04, 0.045, 0.0316666])
+    cases = []
+    mesh = synth.kuhn_box(7, 5, 6, seed=13)
+    cases.append((mesh.P, mesh.T, synth.cube_layout(mesh)))
+    P, T = _pinwheel(n_blades=14, seed=2)
+    cases.append((P, T, np.full(T.shape[0], synth.AIR, dtype=np.int32)))
+    for P, T, tags in cases:
+        edges, t2e, sign, m = make_case(oracle_port, P, T, tags)
+        E = edges.shape[0]
+        nu = np.random.default_rng(T.shape[0]).uniform(0.2, 5.0, T.shape[0]) * material.NU0
+        plan = AssemblyPlan(P, T, t2e, E, tags, sign)
+        assert plan.info.schedule == _lib.SCHEDULE_NZ_ROW_BLOCKS
+        for w in (qw, qw2):
+            plan.set_quadrature(w, curl, val)
+            I, J, V = oracle_port.curl_curl(m, nu, w, curl)
+            ref = oracle_matrix(oracle_port, I, J, V, E, False)
+            plan.set_schedule(_lib.SCHEDULE_NZ_ROW_BLOCKS)
+            k_nz = plan.stiffness(dev(nu))
+            assert_csr_equal(plan.row_ptr, plan.col_idx, k_nz, ref)
+            plan.set_schedule(_lib.SCHEDULE_TWO_PASS)
+            assert torch.equal(plan.stiffness(dev(nu)), k_nz)
