@@ -9,8 +9,13 @@
 //              curl-curl matrix (assemble_curl_curl_kernel_mex.cpp:64-101) and of
 //              the sigma-mass matrix (assemble_mass_kernel_mex.cpp:186-230,
 //              four distinct quadrature points), signed, into shared memory;
-//   phase B -- one thread per row sums both in ascending element order and
-//              writes (K_ab, omega * M_ab): exactly what MATLAB forms for
+//   phase B -- when the mesh has second-contributor bits, phase A already placed
+//              every off-diagonal entry of K and M into one of its nonzero's two
+//              slots (at most two contributions, summed (0 + a) + b, which does not
+//              depend on their order); one thread per row sums the diagonals in
+//              ascending element order and one pass stores the pairs. Otherwise one
+//              thread per row sums all entries in ascending element order. Either
+//              way the pair is (K_ab, omega * M_ab): exactly what MATLAB forms for
 //              K + 1j*omega*M from the two assembled matrices
 //              (FrequencySolver.m:131), where 0*M adds nothing to the real part.
 // The launch is captured once in a CUDA graph and replayed. Block size and CTA

@@ -15,7 +15,13 @@
 //              the residual; the block's contiguous slice of CSR values is then
 //              stored coalesced.
 // HBM traffic is the algorithmic I/O plus the incidence plan; the price is the
-// repeated element-level arithmetic, so the kernel is FP64-bound.
+// repeated element-level arithmetic.
+//
+// Variants further down: k_rowblock_shared evaluates each distinct element of a block
+// once into a shared-memory record; k_rowblock_nz (the default) in addition places
+// every off-diagonal entry straight into its nonzero's slot (an off-diagonal entry has
+// at most two contributions, whose sum does not depend on order) and keeps the per-row
+// element-ordered sum for diagonals and residuals only.
 #include <vector>
 
 #include "common.cuh"
