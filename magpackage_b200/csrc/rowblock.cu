@@ -813,11 +813,19 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_nz(RBArgs A, const int32_
         curls_standard(g, C);
         const unsigned si = (sb >> loc) & 1;
         const double w0 = A.qp.qw[0] * R.adet, nu = R.nu;
+        // the incidence's own curl read from the record by index, in curls_standard's
+        // operation order: (J_p - J_m) r2 for edges 0-2, J_x r2 (negated for edge 4) for 3-5
+        // (J_x - 0 is J_x exactly)
+        const int cp = (0x102 >> (4 * (loc % 3))) & 3, cm = (0x021 >> (4 * (loc % 3))) & 3;
+        const double r2 = R.r2;
         double Cl[3];
-        pick(C, loc, Cl);
-        double bl = R.b[0];
 #pragma unroll
-        for (int j = 1; j < 6; j++) bl = loc == j ? R.b[j] : bl;
+        for (int r = 0; r < 3; r++) {
+            const double jm = loc < 3 ? R.J[3 * r + cm] : 0.0;
+            const double v = (R.J[3 * r + (loc < 3 ? cp : 5 - loc)] - jm) * r2;
+            Cl[r] = loc == 4 ? -v : v;
+        }
+        const double bl = R.b[loc];
         const double rv = flip(qsum_w<Q4>(nu * bl, A.qp, w0, R.adet), si);
         double dv = 0.0;
         if (CALCJ) {
