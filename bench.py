@@ -1,12 +1,12 @@
 """Benchmark: FP64 Newton-Jacobian + residual assembly into CSR (Melem/s).
 
-Workload (the metric's configuration): nonlinear Newton Jacobian and residual
-on a 60x60x60-hexahedron Kuhn cube (1,296,000 tetrahedra, 1,544,580 edges,
-25,002,180 structural nonzeros), node jitter +-0.1h, air/iron/aluminium layout
+Default workload (the metric's largest single-GPU configuration): one Newton step
+of the 110x110x110-hexahedron Kuhn cube (7,986,000 tetrahedra, 9,426,230 edges,
+153,609,830 structural nonzeros), node jitter +-0.1h, air/iron/aluminium layout
 with iron on a 200-point Froehlich B-H spline, edge field A ~ N(0, 1e-3), all
-seeded; synthetic data (the reference publishes no benchmark mesh). One step
-is one assembly: element kernel + fixed-order CSR row reduction, giving the
-Jacobian values and the residual.
+seeded; synthetic data (the reference publishes no benchmark mesh). One step is
+the FP64 Jacobian + residual assembly into the CSR plus BF16 MLP reluctivity
+inference over every element. ``--workload jacobian_60`` is the 60^3 case.
 
   value  -- device-resident inputs (mesh plan built once, A already in HBM);
             CUDA events on the launching stream; inputs are larger than L2.
@@ -15,7 +15,8 @@ Jacobian values and the residual.
             values and the residual back.
   cpu_baseline -- the reference's own C++/OpenMP MEX kernel (compiled
             unchanged into oracle/_ref) plus the restated MATLAB sparse(),
-            on the host cores, one full assembly.
+            on the host cores, one full assembly; its CSR and residual are
+            then the checker of the GPU's output ("parity").
 
 ``--impl reference`` times that CPU path alone as the reference arm.
 Multi-GPU (torchrun): every rank assembles its own instance of the workload
@@ -331,6 +332,11 @@ def run_batched_complex(args):
     print(json.dumps(out), flush=True)
 
 
+# Elements per reference-arm step: a full 110^3 CPU assembly takes ~13 s, so each step
+# times a slab of this many elements (the MEX kernel and sparse() scale linearly).
+REFERENCE_SAMPLE_ELEMS = 1_000_000
+
+
 def build_workload(n: int, seed: int = 0):
     from magpackage_b200 import material, synth
 
@@ -354,13 +360,14 @@ class ClockSampler:
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index: int):
+        import tempfile
+
         self.idx = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"magpackage_b200_clocks_{os.getpid()}_{device_index}.csv")
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -378,8 +385,10 @@ class ClockSampler:
             self.proc.kill()
         self.fh.close()
         sm, smax, reasons = [], [], set()
+        lines = open(self.path).read().splitlines()
+        os.remove(self.path)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -427,28 +436,60 @@ def profiled_traffic(workload):
     return d.get(workload)
 
 
-def cpu_reference(mesh, tags, packed, reps: int = 1):
-    """The reference MEX kernel + restated sparse(), timed on the host cores."""
+def cpu_reference(mesh, tags, packed, reps: int = 1, keep: bool = False, max_elems: int | None = None):
+    """The reference MEX kernel + restated sparse(), timed on the host cores. keep: also
+    return the last repetition's CSR (row_ptr, col_idx, values) and residual. max_elems:
+    time a sample, the first max_elems elements (a slab of whole hexahedron layers), into
+    the full-size matrix."""
     from magpackage_b200 import quadrature
     from oracle.oracle import Port, RefMex, mex_inputs, ref_available
 
     port = Port()
     impl = RefMex() if ref_available() else port
     edges, t2e, sign = port.generate_edges(mesh.T)
-    m = mex_inputs(mesh.P, mesh.T, t2e, sign, tags)
+    k = mesh.num_elements if max_elems is None else min(max_elems, mesh.num_elements)
+    m = mex_inputs(mesh.P, mesh.T[:k], t2e[:k], sign[:k], tags[:k])
     qw, val, curl = quadrature.reference_data(2)
     E = edges.shape[0]
     sol = np.random.default_rng(1).normal(0.0, 1e-3, E)
     times = []
+    out = None
     for _ in range(reps):
         t0 = time.perf_counter()
         I, J, V, Ri, Rv = impl.jacobian(m, sol, qw, curl, packed, True)
         t1 = time.perf_counter()
-        port.sparse_csr(I, J, V, E, drop_zeros=True)
-        port.sparse_vec(Ri, Rv, E)
+        csr = port.sparse_csr(I, J, V, E, drop_zeros=True)
+        vec = port.sparse_vec(Ri, Rv, E)
         t2 = time.perf_counter()
         times.append((t1 - t0, t2 - t1))
-    return times, ("reference" if impl is not port else "port"), os.cpu_count()
+        del csr
+        if keep:  # the structural pattern (no zero dropping), as the library stores it
+            out = (port.sparse_csr(I, J, V, E, drop_zeros=False), vec)
+        del I, J, V, Ri, Rv
+    kind = "reference" if impl is not port else "port"
+    if keep:
+        return times, kind, os.cpu_count(), out
+    return times, kind, os.cpu_count()
+
+
+def parity_against(ref, plan, vals, res):
+    """GPU CSR values and residual against the reference's (bit equality is the test's
+    bound; max relative error per nonzero and Frobenius relative error reported)."""
+    (rp, ci, rv), rres = ref
+    v, r = vals.cpu().numpy(), res.cpu().numpy()
+    same_pattern = bool(np.array_equal(plan.row_ptr.cpu().numpy(), rp) and
+                        np.array_equal(plan.col_idx.cpu().numpy(), ci))
+    out = {"pattern_equal": same_pattern}
+    if same_pattern:
+        nz = rv != 0
+        bits = (v.view(np.int64) == rv.view(np.int64)) | ((v == 0) & (rv == 0))
+        out["values_bit_equal"] = bool(bits.all())
+        out["max_rel"] = float((np.abs(v[nz] - rv[nz]) / np.abs(rv[nz])).max()) if nz.any() else 0.0
+        out["frobenius_rel"] = float(np.linalg.norm(v - rv) / max(np.linalg.norm(rv), 1e-300))
+        rz = rres != 0
+        out["residual_bit_equal"] = bool(((r.view(np.int64) == rres.view(np.int64)) | ((r == 0) & (rres == 0))).all())
+        out["residual_max_rel"] = float((np.abs(r[rz] - rres[rz]) / np.abs(rres[rz])).max()) if rz.any() else 0.0
+    return out
 
 
 def run_reference_arm(args, rank, world, workload):
@@ -457,19 +498,22 @@ def run_reference_arm(args, rank, world, workload):
     n, desc = WORKLOADS[workload]
     mesh, tags, packed = build_workload(n)
     ne = mesh.num_elements
-    times, kind, cores = cpu_reference(mesh, tags, packed, reps=args.warmup + args.steps)
+    sample = min(ne, REFERENCE_SAMPLE_ELEMS)
+    times, kind, cores = cpu_reference(mesh, tags, packed, reps=args.warmup + args.steps, max_elems=sample)
     timed = times[args.warmup:]
     total = sum(a + b for a, b in timed)
-    v = ne * len(timed) / total / 1e6
+    v = sample * len(timed) / total / 1e6
     out = {"metric": "Jacobian assembly Melem/s (FP64 CSR)", "value": v, "unit": "Melem/s",
            "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": total / len(timed) * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": {"workload": desc, "elements": ne},
            "cpu_baseline": {"value": v, "unit": "Melem/s", "cores": cores, "kind": kind,
-                            "sample": f"full {workload} assembly per step: MEX kernel "
-                                      f"{1e3 * statistics.median(a for a, _ in timed):.0f} ms + sparse() "
-                                      f"{1e3 * statistics.median(b for _, b in timed):.0f} ms"},
+                            "sample": (f"full {workload} assembly per step" if sample == ne else
+                                       f"per step the first {sample} of the {ne} tets (whole hexahedron "
+                                       "layers) into the full-size matrix") +
+                                      f": MEX kernel {1e3 * statistics.median(a for a, _ in timed):.0f} ms "
+                                      f"+ sparse() {1e3 * statistics.median(b for _, b in timed):.0f} ms"},
            "e2e": {"value": v, "unit": "Melem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -480,7 +524,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="jacobian_60",
+    ap.add_argument("--workload", default="jacobian_110_mlp",
                     choices=sorted(WORKLOADS) + ["batched_complex", "transient", "hbfem", "stiffness", "mex"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--schedule", default="nz-row-blocks",
@@ -663,13 +707,18 @@ def main():
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and not args.no_cpu_baseline:
-        times, kind, cores = cpu_reference(mesh, tags, packed, reps=1)
+        plan.jacobian(sol, vals, res)  # the timed call's output, kept for the check below
+        torch.cuda.synchronize()
+        times, kind, cores, ref = cpu_reference(mesh, tags, packed, reps=1, keep=True)
         k, s = times[0]
         cpu = {"value": ne / (k + s) / 1e6, "unit": "Melem/s", "cores": cores, "kind": kind,
                "sample": f"one full {args.workload} assembly ({ne} tets): MEX kernel {k * 1e3:.0f} ms "
                          f"+ sparse() {s * 1e3:.0f} ms, OpenMP on all host threads"}
+        parity = parity_against(ref, plan, vals, res)
+        parity["checker"] = f"{kind} MEX kernel + restated sparse(), same mesh and state"
+        del ref
 
     if rank == 0:
         b_elem = algorithmic_bytes_per_elem(ne, mesh.num_nodes, E, nnz)
@@ -710,6 +759,7 @@ def main():
             "gpu_launches": ((1 if single else 2) + (1 if with_mlp else 0)) * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "parity": parity,
         }
         if with_mlp:
             out["split_ms"] = {"assembly": ms_asm, "mlp_inference": ms_mlp,

@@ -264,8 +264,13 @@ int mag_mlp_gradient(mag_mlp *mlp, const float *d_feats, const float *d_target, 
 /* One Adam step (lr, betas 0.9/0.999) on the mean-squared error of a minibatch. */
 int mag_mlp_train_step(mag_mlp *mlp, const float *d_feats, const float *d_target, int64_t rows,
                        float lr, float *d_y, float *d_z, void *stream);
-/* Synchronise; MAG_E_TIMEOUT if a tensor-core completion wait gave up. */
+/* Synchronise; MAG_E_TIMEOUT if a tensor-core completion wait gave up since the last
+ * check (the status is cleared once reported). The outputs of that call are incomplete. */
 int mag_mlp_check(mag_mlp *mlp, void *stream);
+/* Polls a kernel makes on a tensor-core completion before it gives up (then it waits
+ * for the MMAs it issued, frees its tensor memory, records MAG_E_TIMEOUT and returns);
+ * 0 restores the default bound (about a second). Small values exist to test that path. */
+int mag_mlp_set_spin_limit(mag_mlp *mlp, int64_t polls);
 
 /* ---- sparse algebra for the Newton driver ------------------------------------
  * CSR arguments: d_row_ptr [n+1] int64, d_col_idx [nnz] int32, d_vals [nnz]. */
@@ -400,9 +405,12 @@ int mag_sparse_destroy(mag_sparse *sp);
  * go to a static device array inside the library (Ne <= 32768, nmat <= 64,
  * nbrk <= 4096, ncoe <= 16384; larger sizes return MAG_E_UNSUPPORTED), which
  * every GPU that loads the library holds until exit. The first call on a
- * device looks up that array's address, so make it before any stream capture.
- * Calls share the array: calls that overlap on the GPU race and must be
- * serialised. Synchronises `stream` to report index errors. */
+ * device looks up that array's address, so make it before any stream capture;
+ * with lazy module loading (CUDA's default) that first call is also when the
+ * array is committed on the device, and it can fail with MAG_E_CUDA when the
+ * device has no memory left, so make it early. Calls share the array: calls
+ * that overlap on the GPU race and must be serialised. Synchronises `stream` to
+ * report index errors (MAG_E_RANGE; the offending elements' values are NaN). */
 int mag_mex_jacobian_noalloc(const double *d_P, int64_t Nn, const double *d_T, int64_t Ne,
                              const double *d_Dofs, const double *d_Signs, const double *d_Tags,
                              const double *d_SolA, int64_t Ndof, const double *Qw, int nq,

@@ -84,6 +84,7 @@ _PROTOS = {
     "mag_mlp_gradient": ([_vp, _vp, _vp, _i64, C.c_float, _vp, _vp, _vp, _vp], _int),
     "mag_mlp_train_step": ([_vp, _vp, _vp, _i64, C.c_float, _vp, _vp, _vp], _int),
     "mag_mlp_check": ([_vp, _vp], _int),
+    "mag_mlp_set_spin_limit": ([_vp, _i64], _int),
     "mag_csr_drop_zeros": ([_vp, _vp, _vp, _i64, _vp, _vp, _vp, C.POINTER(_i64), _vp], _int),
     "mag_mex_jacobian": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _i64, _dp, _int, _dp, _dp, _dp,
                           _dp, _int, _dp, _int, _dp, _int, _dp, _dp, _dp, _int, _dp, _dp, _dp, _dp,

@@ -969,6 +969,7 @@ struct mag_mlp {
     __nv_bfloat16 *ops = nullptr;
     int *err = nullptr;
     int grid = 0, step = 0;
+    long long spin_limit = 0;
 };
 
 namespace {
@@ -1048,7 +1049,8 @@ int mag_mlp_forward(mag_mlp *n, const float *d_feats, int64_t rows, float *d_y, 
         set_error("mag_mlp_forward: bad arguments");
         return MAG_E_ARG;
     }
-    MlpForwardArgs a{d_feats, rows, n->params, n->ops, d_y, d_z, nullptr, nullptr, 0, 0, 0, 0, n->err};
+    MlpForwardArgs a{d_feats, rows, n->params, n->ops, d_y, d_z, nullptr, nullptr, 0, 0, 0, 0, n->err,
+                     n->spin_limit};
     return mlp_forward(a, mlp_grid(rows, 4 * n->grid), (cudaStream_t)stream);
 }
 
@@ -1059,7 +1061,7 @@ int mag_mlp_predict_nu(mag_mlp *n, const float *d_feats, int64_t rows, const int
         return MAG_E_ARG;
     }
     MlpForwardArgs a{d_feats, rows, n->params, n->ops, nullptr, nullptr, d_nu, d_rows, y_scale, y_shift,
-                     nu_min, nu_max, n->err};
+                     nu_min, nu_max, n->err, n->spin_limit};
     return mlp_forward(a, mlp_grid(rows, 4 * n->grid), (cudaStream_t)stream);
 }
 
@@ -1070,10 +1072,11 @@ int mag_mlp_gradient(mag_mlp *n, const float *d_feats, const float *d_target, in
         return MAG_E_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    MlpForwardArgs fa{d_feats, rows, n->params, n->ops, d_y, d_z, nullptr, nullptr, 0, 0, 0, 0, n->err};
+    MlpForwardArgs fa{d_feats, rows, n->params, n->ops, d_y, d_z, nullptr, nullptr, 0, 0, 0, 0, n->err,
+                      n->spin_limit};
     MAG_TRY(mlp_forward(fa, mlp_grid(rows, 4 * n->grid), s));
     MlpBackwardArgs ba{d_feats, d_z, d_y, d_target, rows, loss_scale, n->params, n->ops, n->partial,
-                       d_grad ? d_grad : n->grad, n->err};
+                       d_grad ? d_grad : n->grad, n->err, n->spin_limit};
     return mlp_backward(ba, mlp_grid(rows, n->grid), s);
 }
 
@@ -1089,12 +1092,25 @@ int mag_mlp_train_step(mag_mlp *n, const float *d_feats, const float *d_target, 
 int mag_mlp_check(mag_mlp *n, void *stream) {
     if (!n) return MAG_E_ARG;
     int h = 0;
-    MAG_CUDA_TRY(cudaMemcpyAsync(&h, n->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
-    MAG_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    cudaStream_t s = (cudaStream_t)stream;
+    MAG_CUDA_TRY(cudaMemcpyAsync(&h, n->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MAG_CUDA_TRY(cudaStreamSynchronize(s));
     if (h) {
+        // reported once: the word is cleared so that later calls start clean
+        MAG_CUDA_TRY(cudaMemsetAsync(n->err, 0, sizeof(int), s));
+        MAG_CUDA_TRY(cudaStreamSynchronize(s));
         set_error("an MLP kernel's bounded wait on its tensor-core completion gave up");
         return MAG_E_TIMEOUT;
     }
+    return MAG_OK;
+}
+
+int mag_mlp_set_spin_limit(mag_mlp *n, int64_t polls) {
+    if (!n || polls < 0) {
+        set_error("mag_mlp_set_spin_limit: bad arguments");
+        return MAG_E_ARG;
+    }
+    n->spin_limit = (long long)polls;
     return MAG_OK;
 }
 

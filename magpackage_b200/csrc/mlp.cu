@@ -78,9 +78,24 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Bounded wait on phase `parity`; returns false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// Bounded wait on phase `parity`; returns false if it gave up. limit = 0: kMbarSpin
+// polls of the potentially blocking try_wait; limit > 0: that many polls of the
+// non-blocking test_wait (a caller-set limit, small in tests, that really runs out).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit = 0) {
     uint32_t done = 0;
+    if (limit > 0) {
+        for (long long i = 0; i < limit; i++) {
+            asm volatile(
+                "{\n\t.reg .pred P1;\n\t"
+                "mbarrier.test_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                "selp.b32 %0, 1, 0, P1;\n\t}"
+                : "=r"(done)
+                : "r"(smem_u32(bar)), "r"(parity)
+                : "memory");
+            if (done) return true;
+        }
+        return false;
+    }
     for (long long i = 0; i < kMbarSpin; i++) {
         asm volatile(
             "{\n\t.reg .pred P1;\n\t"
@@ -213,8 +228,12 @@ __device__ __forceinline__ void tmem_free(Smem &S) {
     }
 }
 
-// One layer: D = act * W^T; waits for completion; returns false on timeout.
-__device__ __forceinline__ bool run_layer(Smem &S, const __nv_bfloat16 *W, int K, uint32_t &phase) {
+// One layer: D = act * W^T; waits for completion; returns false on timeout. A wait
+// that gives up first drains: the issued MMAs still read shared memory and write TMEM,
+// so the kernel waits for their commit (default bound) before it leaves the tile loop
+// and frees TMEM.
+__device__ __forceinline__ bool run_layer(Smem &S, const __nv_bfloat16 *W, int K, uint32_t &phase,
+                                          long long limit) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // smem writes -> tensor core
     tc_fence_before();
     __syncthreads();
@@ -222,7 +241,8 @@ __device__ __forceinline__ bool run_layer(Smem &S, const __nv_bfloat16 *W, int K
         tc_fence_after();
         mma_issue(S.tmem, S.act, W, K, &S.bar);
     }
-    bool ok = mbar_wait(&S.bar, phase);
+    bool ok = mbar_wait(&S.bar, phase, limit);
+    if (!ok) mbar_wait(&S.bar, phase);
     phase ^= 1u;
     tc_fence_after();
     // block-uniform outcome, so every thread leaves the tile loop together
@@ -277,13 +297,13 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
         // layer 1
         // (a completed MMA has read its input image; the next layer's issue barrier orders
         // this thread's TMEM reads and image writes before the next MMA)
-        if (!run_layer(S, W1, 16, phase)) break;
+        if (!run_layer(S, W1, 16, phase, a.spin_limit)) break;
         hidden_epilogue(S.tmem, sb1, S.act, t, zr);
         // layer 2
-        if (!run_layer(S, W2, kH, phase)) break;
+        if (!run_layer(S, W2, kH, phase, a.spin_limit)) break;
         hidden_epilogue(S.tmem, sb2, S.act, t, zr ? zr + kH : nullptr);
         // layer 3 and the 64 -> 1 output, 16 columns at a time
-        if (!run_layer(S, W3, kH, phase)) break;
+        if (!run_layer(S, W3, kH, phase, a.spin_limit)) break;
         float y = 0.0f;
 #pragma unroll
         for (int c = 0; c < kH; c += 16) {
@@ -402,7 +422,7 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp_backward(MlpBackwardArgs a) {
         __syncthreads();
         weight_grads(B, kH, G + oW3, G + ob3);
         put_row64(S.act, t, dz);
-        if (!run_layer(S, W3T, kH, phase)) break;
+        if (!run_layer(S, W3T, kH, phase, a.spin_limit)) break;
         tmem_row(S.tmem, dh);
         tc_fence_before();
         __syncthreads();
@@ -415,7 +435,7 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp_backward(MlpBackwardArgs a) {
         __syncthreads();
         weight_grads(B, kH, G + oW2, G + ob2);
         put_row64(S.act, t, dz);
-        if (!run_layer(S, W2T, kH, phase)) break;
+        if (!run_layer(S, W2T, kH, phase, a.spin_limit)) break;
         tmem_row(S.tmem, dh);
         tc_fence_before();
         __syncthreads();

@@ -24,6 +24,7 @@ struct MlpForwardArgs {
     const int32_t *rows;
     double y_scale, y_shift, nu_min, nu_max;
     int *err;
+    long long spin_limit;   // polls before a tensor-core wait gives up; 0 = the default bound
 };
 
 struct MlpBackwardArgs {
@@ -35,6 +36,7 @@ struct MlpBackwardArgs {
     float *grad_partial;    // [grid][kMlpParams]
     float *grad;            // [kMlpParams]
     int *err;
+    long long spin_limit;
 };
 
 size_t mlp_forward_smem();

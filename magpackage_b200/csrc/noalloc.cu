@@ -19,8 +19,13 @@
 //
 // The first call on each device looks up the array's device address with
 // cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture begins. Nothing here calls cudaMalloc,
-// cudaFree or any allocating library routine.
+// first call before any stream capture begins. With CUDA's lazy module loading
+// (the default) the array is committed on a device at that first call, not when
+// the library is loaded, so a first call made under a tight memory budget can
+// fail for lack of device memory (MAG_E_CUDA); make it early. Nothing here calls
+// cudaMalloc, cudaFree or any allocating library routine.
+// An element that fails the input checks makes the call return MAG_E_RANGE and
+// leaves NaN in its triplet values and residual entries.
 #include <mutex>
 
 #include "common.cuh"
@@ -87,11 +92,20 @@ __global__ void __launch_bounds__(128) k_na_elems(NaArgs a, QuadParams qp, Mater
                                                   double *__restrict__ blocks, int *__restrict__ err) {
     int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= a.ne) return;
+    double *dst = blocks + e * kScratchPerElem;
+    // an element that fails a check flags the call and leaves NaN in its block, so the
+    // triplets copied from it are visibly invalid rather than the previous call's values
+    auto reject = [&]() {
+        atomicOr(err, 1);
+        const double nan = __longlong_as_double(0x7FF8000000000000LL);
+        const double row[6] = {nan, nan, nan, nan, nan, nan};
+        for (int i = 0; i < 6; i++) elem::store_row(dst + i * kScratchStride, row, nan);
+    };
     int node[4];
     for (int k = 0; k < 4; k++) {
         double v = a.T[4 * e + k];
         if (!(v >= 1.0 && v < (double)a.nn + 1.0)) {
-            atomicOr(err, 1);
+            reject();
             return;
         }
         node[k] = (int)v - 1;
@@ -101,7 +115,7 @@ __global__ void __launch_bounds__(128) k_na_elems(NaArgs a, QuadParams qp, Mater
     for (int k = 0; k < 6; k++) {
         double v = a.Dofs[6 * e + k], s = a.Signs[6 * e + k];
         if (!(v > -1.0 && v < (double)a.ndof + 1.0) || (s != 1.0 && s != -1.0)) {
-            atomicOr(err, 1);
+            reject();
             return;
         }
         d[k] = (int)v - 1;
@@ -109,15 +123,16 @@ __global__ void __launch_bounds__(128) k_na_elems(NaArgs a, QuadParams qp, Mater
     }
     double tv = a.Tags[e];
     if (!(tv >= 1.0 && tv < (double)a.nmat + 1.0)) {
-        atomicOr(err, 1);
+        reject();
         return;
     }
     int tag = (int)tv;
     double4 v[4];
     for (int k = 0; k < 4; k++) {
-        v[k] = make_double4(a.P[3 * node[k]], a.P[3 * node[k] + 1], a.P[3 * node[k] + 2], 0.0);
+        const int64_t p = 3 * (int64_t)node[k];
+        v[k] = make_double4(a.P[p], a.P[p + 1], a.P[p + 2], 0.0);
         if (!isfinite(v[k].x) || !isfinite(v[k].y) || !isfinite(v[k].z)) {
-            atomicOr(err, 1);
+            reject();
             return;
         }
     }
@@ -136,7 +151,6 @@ __global__ void __launch_bounds__(128) k_na_elems(NaArgs a, QuadParams qp, Mater
     for (int i = 0; i < 6; i++) av[i] = d[i] >= 0 ? elem::flip(a.Sol[d[i]], (sb >> i) & 1) : 0.0;
     double res[6], K[6][6];
     elem::jacobian_block<CALCJ, STDCURL>(g, av, tag, qp, mp, res, K);
-    double *dst = blocks + e * kScratchPerElem;
     for (int i = 0; i < 6; i++) {
         double row[6];
         for (int j = 0; j < 6; j++) row[j] = CALCJ ? elem::flip(K[i][j], ((sb >> i) ^ (sb >> j)) & 1) : 0.0;

@@ -91,6 +91,10 @@ class MLP:
     def check(self):
         _lib.check(self._lib.mag_mlp_check(self._h, _lib.stream_ptr()))
 
+    def set_spin_limit(self, polls: int = 0):
+        """Polls before a tensor-core completion wait gives up (0: the default bound)."""
+        _lib.check(self._lib.mag_mlp_set_spin_limit(self._h, int(polls)))
+
     def close(self):
         if getattr(self, "_h", None):
             self._lib.mag_mlp_destroy(self._h)

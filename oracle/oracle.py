@@ -337,3 +337,35 @@ class RefMex(_Lib):
 
 def ref_available() -> bool:
     return os.path.exists(REF_SO)
+
+
+def element_b(P, T0, dofs0, sign, sol):
+    """PostProcessor.computeElementB (src/post/PostProcessor.m:64-126), restated in numpy.
+
+    Per element: J = [x2-x1, x3-x1, x4-x1] and detJ by first-row cofactors
+    (src/utils/compute_jacobian_tet.m:14-28); reference curls C_ref(e,:) =
+    2 * cross(grad L_i, grad L_j) for the local edges (1,2),(1,3),(1,4),(2,3),(2,4),(3,4)
+    (src/shape_functions/nedelec_tet_p1.m:28-51); C_phy = (C_ref * J') / detJ;
+    B = C_phy' * (A(dofs) .* signs). MATLAB evaluates the two products with BLAS, whose
+    summation order is unspecified, so this restatement pins B to rounding level, not to
+    the bit. P (Nn,3), T0 (Ne,4) and dofs0 (Ne,6) 0-based, sign (Ne,6) +-1, sol [Ndof].
+    Returns B (Ne,3) and, per element, the bound sum_e |C_phy(e,:)| |a_e| that scales its
+    rounding error.
+    """
+    P = np.asarray(P, dtype=np.float64)
+    T0 = np.asarray(T0, dtype=np.int64)
+    G = np.array([[-1.0, -1.0, -1.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+    pairs = ((0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3))
+    C_ref = np.array([2.0 * np.cross(G[i], G[j]) for i, j in pairs])  # (6, 3)
+    x1, x2, x3, x4 = (P[T0[:, k]] for k in range(4))
+    d1, d2, d3 = x2 - x1, x3 - x1, x4 - x1
+    J = np.stack([d1, d2, d3], axis=2)  # J[:, r, c] = d_c[r]
+    det = (d1[:, 0] * (d2[:, 1] * d3[:, 2] - d2[:, 2] * d3[:, 1])
+           - d1[:, 1] * (d2[:, 0] * d3[:, 2] - d2[:, 2] * d3[:, 0])
+           + d1[:, 2] * (d2[:, 0] * d3[:, 1] - d2[:, 1] * d3[:, 0]))
+    C_phy = np.einsum("ec,nrc->ner", C_ref, J) * (1.0 / det)[:, None, None]  # (Ne, 6, 3)
+    dofs0 = np.asarray(dofs0, dtype=np.int64)
+    a = np.where(dofs0 >= 0, np.asarray(sol, dtype=np.float64)[np.maximum(dofs0, 0)], 0.0) * sign
+    B = np.einsum("ner,ne->nr", C_phy, a)
+    scale = np.einsum("ner,ne->nr", np.abs(C_phy), np.abs(a))
+    return B, scale

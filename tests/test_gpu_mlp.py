@@ -63,3 +63,29 @@ def test_training_reduces_loss():
     y1, _ = net.forward(xd)
     l1 = float(((y1 - td) ** 2).mean())
     assert l1 < 0.1 * l0, (l0, l1)
+
+
+def test_bounded_wait_gives_up_and_recovers():
+    """A tensor-core completion wait limited to one non-blocking poll runs out (the MMA
+    is still in flight right after it is issued): the kernels drain their MMAs, free tensor
+    memory, report MAG_E_TIMEOUT through mag_mlp_check once, and the next call with the
+    default bound is exact again."""
+    from magpackage_b200 import _lib
+
+    p, x, t = _case(8192, 3)
+    net = MLP(p)
+    xd, td = torch.as_tensor(x, device="cuda"), torch.as_tensor(t, device="cuda")
+    net.set_spin_limit(1)
+    net.forward(xd)
+    with pytest.raises(_lib.MagError) as ei:
+        net.check()
+    assert ei.value.code == -5  # MAG_E_TIMEOUT
+    net.gradient(xd, td, 2.0 / len(t))
+    with pytest.raises(_lib.MagError) as ei:
+        net.check()
+    assert ei.value.code == -5
+    net.set_spin_limit(0)
+    y, _ = net.forward(xd)
+    net.check()  # the status was cleared when it was reported
+    y_ref, _ = mlp_ref.forward(p, x)
+    assert np.max(np.abs(y.cpu().numpy() - y_ref)) <= 2e-3 * (1 + np.max(np.abs(y_ref)))

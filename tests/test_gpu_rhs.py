@@ -95,3 +95,30 @@ def test_assembler_winding_surface(oracle_port):
     with pytest.raises(ValueError):
         w2.set_direction_field(np.zeros((3, 3)))
         asm.assemble_winding(w2)
+
+
+@pytest.mark.parametrize("flip", [False, True])
+def test_element_b_matches_postprocessor(oracle_port, flip):
+    """mag_element_b against PostProcessor.computeElementB restated (PostProcessor.m:64-126):
+    B per element within 1e-12 of its rounding scale (MATLAB's BLAS products have no fixed
+    summation order, so this is a tolerance, not a bit comparison), |B|^2 = B.B bit for bit;
+    with the mesh's own signs and with explicitly flipped ones."""
+    from oracle.oracle import element_b
+    from test_oracle import uniform_field_edges
+
+    mesh = synth.kuhn_box(9, 7, 8, seed=5)
+    tags = synth.cube_layout(mesh)
+    edges, t2e, sign = oracle_port.generate_edges(mesh.T)
+    if flip:
+        sign = sign.copy()
+        sign[::3] *= -1
+    E = edges.shape[0]
+    plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
+    rng = np.random.default_rng(4)
+    for sol in (rng.normal(0, 1e-2, E), uniform_field_edges(mesh.P, edges, np.array([0.2, 0.5, -1.1]))):
+        b, bsq = plan.element_b(torch.as_tensor(sol, device="cuda"))
+        b, bsq = b.cpu().numpy(), bsq.cpu().numpy()
+        B, scale = element_b(mesh.P, mesh.T, t2e, sign, sol)
+        assert np.all(np.abs(b - B) <= 1e-12 * scale + 1e-300)
+        assert bits_equal(bsq, (b[:, 0] * b[:, 0] + b[:, 1] * b[:, 1]) + b[:, 2] * b[:, 2])
+    plan.close()

@@ -206,3 +206,27 @@ def test_hbfem_single_dc_harmonic_is_the_static_residual(oracle_port):
     st = oracle_port.sparse_vec(Ri, Rv, E)
     assert np.abs(hb - st).max() <= 1e-13 * np.abs(st).max()
     assert np.all(Rim == 0.0)
+
+
+def uniform_field_edges(P, edges, B0):
+    """Edge dofs of A = B0 x x / 2 (curl A = B0): the line integral along each global edge,
+    oriented from its first to its second node, exact for a linear field."""
+    p, q = P[edges[:, 0]], P[edges[:, 1]]
+    return 0.5 * np.einsum("ij,ij->i", np.cross(B0, 0.5 * (p + q)), q - p)
+
+
+def test_element_b_restatement_patch_test(oracle_port):
+    """PostProcessor.computeElementB restated: a uniform field is reproduced in every
+    element (Nedelec elements contain the constant curls exactly)."""
+    from oracle.oracle import element_b
+
+    mesh = synth.kuhn_box(5, 4, 3, seed=7)
+    edges, t2e, sign = oracle_port.generate_edges(mesh.T)
+    B0 = np.array([0.3, -1.2, 0.7])
+    sol = uniform_field_edges(mesh.P, edges, B0)
+    B, scale = element_b(mesh.P, mesh.T, t2e, sign, sol)
+    assert np.all(np.abs(B - B0) <= 1e-12 * scale)
+    # a gradient field (edge differences of a nodal potential) has zero curl
+    phi = np.random.default_rng(3).normal(size=mesh.num_nodes)
+    B, scale = element_b(mesh.P, mesh.T, t2e, sign, phi[edges[:, 1]] - phi[edges[:, 0]])
+    assert np.all(np.abs(B) <= 1e-12 * scale)
