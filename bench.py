@@ -174,9 +174,10 @@ def run_stiffness(args):
 
 def run_mex(args):
     """The MATLAB drop-in path at 60^3, per call: host arrays in the reference's MEX layout
-    through the C ABI, the mesh uploaded and planned inside every call (as a gateway call
-    does), and either the reference's triplets or MATLAB's compressed-column sparse matrix
-    plus the residual back on the host. Wall clock; the calls synchronise."""
+    through the C ABI (as a gateway call passes them), and either the reference's triplets
+    or MATLAB's compressed-column sparse matrix plus the residual back on the host. The
+    first call converts and caches the mesh; later calls with the same arrays find it.
+    Wall clock; the calls synchronise."""
     import ctypes as C
 
     import torch
@@ -224,6 +225,10 @@ def run_mex(args):
 
     steps, warm = min(args.steps, 5), min(args.warmup, 2)
     res = {}
+    _lib.check(L.mag_mex_cache_clear())
+    t0 = time.perf_counter()
+    sparse()  # first call: the mesh is converted, planned and cached
+    first_ms = (time.perf_counter() - t0) * 1e3
     for name, fn in (("triplets", triplets), ("sparse", sparse)):
         for _ in range(warm):
             fn()
@@ -244,9 +249,12 @@ def run_mex(args):
            "value": ne / (res["sparse"] * 1e-3) / 1e6, "unit": "Melem/s", "n_gpus": 1, "steps": steps,
            "warmup": warm, "ms_per_step": res["sparse"], "higher_is_better": True, "dtype": "f64",
            "data": "synthetic",
-           "config": {"workload": "Newton Jacobian + residual, 60^3 Kuhn cube (1.296M tets), MEX layout, "
-                                  "mesh uploaded and planned in every call",
-                      "elements": ne, "nnz_stored": nnz, "triplet_call_ms": res["triplets"],
+           "config": {"workload": "Newton Jacobian + residual, 60^3 Kuhn cube (1.296M tets), MEX layout; the "
+                                  "mesh is converted on the first call and found in the library's cache "
+                                  "(content hash) on the timed calls, which upload SolA and copy out the "
+                                  "sparse matrix and residual",
+                      "elements": ne, "nnz_stored": nnz, "first_call_ms": first_ms,
+                      "triplet_call_ms": res["triplets"],
                       "triplet_bytes_out": int(3 * I.nbytes + 2 * Ri.nbytes)},
            "cpu_baseline": cpu}
     print(json.dumps(out), flush=True)
@@ -527,9 +535,8 @@ def main():
     ap.add_argument("--workload", default="jacobian_110_mlp",
                     choices=sorted(WORKLOADS) + ["batched_complex", "transient", "hbfem", "stiffness", "mex"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--schedule", default="nz-row-blocks",
-                    choices=["shared-row-blocks", "nz-row-blocks", "staged-row-blocks", "row-blocks", "l2-ring",
-                             "two-pass"],
+    ap.add_argument("--schedule", default="tile-blocks",
+                    choices=["tile-blocks", "shared-row-blocks", "nz-row-blocks", "row-blocks", "two-pass"],
                     help="Jacobian assembly schedule (all give identical bits)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -577,10 +584,9 @@ def main():
     E = int(edges.shape[0])
     plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
     plan.set_materials(packed)
-    sched_id = {"shared-row-blocks": _lib.SCHEDULE_SHARED_ROW_BLOCKS,
+    sched_id = {"tile-blocks": _lib.SCHEDULE_TILE_BLOCKS, "shared-row-blocks": _lib.SCHEDULE_SHARED_ROW_BLOCKS,
                 "nz-row-blocks": _lib.SCHEDULE_NZ_ROW_BLOCKS,
-                "staged-row-blocks": _lib.SCHEDULE_STAGED_ROW_BLOCKS,
-                "row-blocks": _lib.SCHEDULE_ROW_BLOCKS, "l2-ring": _lib.SCHEDULE_L2_RING,
+                "row-blocks": _lib.SCHEDULE_ROW_BLOCKS,
                 "two-pass": _lib.SCHEDULE_TWO_PASS}[args.schedule]
     plan.set_schedule(sched_id)
     single = sched_id != _lib.SCHEDULE_TWO_PASS
@@ -733,20 +739,22 @@ def main():
             "config": {"workload": desc, "elements": ne, "edges": E, "nnz": nnz,
                        "l2": "inputs larger than L2 (per-step working set > 700 MB)",
                        "parallelism": f"{world} independent instance(s)",
-                       "shared_blocks": plan.info.shared_blocks, "shared_staged": plan.info.shared_staged,
-                       "schedule": {_lib.SCHEDULE_NZ_ROW_BLOCKS: "row blocks with shared elements; "
+                       "shared_blocks": plan.info.shared_blocks,
+                       "tile_blocks": plan.info.tile_blocks,
+                       "element_evaluations_per_element": round(plan.info.tile_evals_per_elem, 4),
+                       "plan_build_ms": round(plan.info.tile_plan_ms, 1),
+                       "schedule": {_lib.SCHEDULE_TILE_BLOCKS: "spatial tiles of 4x4x4 node layers: one CTA per "
+                                                               "block of whole rows, one thread per incident "
+                                                               "element, off-diagonal entries placed in colour "
+                                                               "phases, diagonals and residuals summed per row",
+                                    _lib.SCHEDULE_NZ_ROW_BLOCKS: "row blocks with shared elements; "
                                                                  "off-diagonal entries placed by their "
                                                                  "incidences, one pass over the nonzeros",
-                                    _lib.SCHEDULE_STAGED_ROW_BLOCKS: "row blocks with shared elements, the "
-                                                                     "block's nodes and edge values staged in "
-                                                                     "shared memory first",
                                     _lib.SCHEDULE_SHARED_ROW_BLOCKS: "row blocks: one launch, no scratch, "
                                                                      "each block's distinct elements "
                                                                      "evaluated once in shared memory",
                                     _lib.SCHEDULE_ROW_BLOCKS: "row blocks: one launch, per-row element "
                                                               "recompute, no scratch",
-                                    _lib.SCHEDULE_L2_RING: "one persistent launch, L2 scratch ring of "
-                                                           f"{plan.info.fused_ring_tiles} tiles",
                                     _lib.SCHEDULE_TWO_PASS: "two passes (element kernel + row "
                                                             "reduction)"}[sched_id]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -52,29 +52,38 @@ typedef struct {
     int32_t wide_positions; /* 1 if some row exceeds 31 entries */
     int32_t signs_derived;  /* 1 if signs equal the Mesh.m:134 rule and are not stored */
     int32_t schedule;       /* MAG_SCHEDULE_* used by the Jacobian assembly */
-    int32_t fused_ring_tiles; /* element tiles the L2 scratch ring holds (MAG_SCHEDULE_L2_RING) */
-    int32_t fused_grid;     /* co-resident CTAs of that launch */
+    int32_t tile_blocks;    /* CTA blocks of MAG_SCHEDULE_TILE_BLOCKS (0 = not available) */
+    int32_t tile_colors;    /* largest number of element colour classes in one of its blocks */
     int64_t device_bytes;   /* memory held by the handle */
     int32_t shared_blocks;  /* row blocks of MAG_SCHEDULE_SHARED_ROW_BLOCKS (0 = not available) */
-    int32_t shared_staged;  /* 1 once MAG_SCHEDULE_STAGED_ROW_BLOCKS has been selected (tables built) */
+    int32_t reserved0;      /* 0 */
     int32_t nz_pass;        /* 1 if MAG_SCHEDULE_NZ_ROW_BLOCKS is available for this mesh */
+    double tile_evals_per_elem; /* element evaluations per element and assembly of the tile schedule */
+    double tile_plan_ms;    /* host time to build its plan */
 } mag_mesh_info;
 
 /* Jacobian assembly schedules; all give identical bits. */
 #define MAG_OPTION_SCHEDULE 1
 #define MAG_SCHEDULE_TWO_PASS 0   /* element kernel + row reduction through an HBM scratch slab */
-#define MAG_SCHEDULE_L2_RING 1    /* one persistent launch, scratch ring sized to stay in L2 */
+#define MAG_SCHEDULE_RETIRED_1 1  /* retired (a persistent launch over an L2 scratch ring); rejected */
 #define MAG_SCHEDULE_ROW_BLOCKS 2 /* one launch, no scratch: per-row element recompute */
 #define MAG_SCHEDULE_SHARED_ROW_BLOCKS 3 /* as 2, each block's distinct elements evaluated once in shared
                                             memory (standard curl table, else runs as 2) */
-#define MAG_SCHEDULE_STAGED_ROW_BLOCKS 4 /* as 3, the block's distinct nodes and edge values first gathered
-                                            once into shared memory (measured slower than 3 on B200); its
-                                            tables are built when it is first selected */
+#define MAG_SCHEDULE_RETIRED_4 4  /* retired (as 3 with the block's nodes and edge values staged first:
+                                     slower than 3); rejected */
 #define MAG_SCHEDULE_NZ_ROW_BLOCKS 5     /* as 3, each off-diagonal entry placed by its (at most two)
                                             contributing incidences and the block's nonzeros stored in one
                                             pass; only diagonals and residuals are summed per row (meshes
                                             whose off-diagonal entries have more than two contributions,
-                                            e.g. repeated dofs, run as 3). The default when available */
+                                            e.g. repeated dofs, run as 3) */
+#define MAG_SCHEDULE_TILE_BLOCKS 6 /* one launch, no scratch: blocks of whole rows whose edges start in a
+                                      4x4x4-layer spatial tile of nodes; one thread per incident element
+                                      (about 1.5 evaluations per element) writes its rows' off-diagonal
+                                      entries into the block's values in colour phases (no two elements of
+                                      a colour share an entry), diagonals and residuals are summed per row
+                                      in element order. Needs rows of at most 31 entries and off-diagonal
+                                      entries of at most two contributions (standard curl table; else the
+                                      row-block schedules run). The default when available */
 
 /* ---- library ------------------------------------------------------------ */
 
@@ -108,8 +117,10 @@ int mag_mesh_destroy(mag_mesh *mesh);
 int mag_mesh_get_info(const mag_mesh *mesh, mag_mesh_info *info);
 /* Handle options (MAG_OPTION_*). */
 int mag_mesh_set_option(mag_mesh *mesh, int option, int64_t value);
-/* Synchronise `stream` and report whether the last assemblies completed: MAG_E_TIMEOUT
- * if a bounded device-side wait of the L2-ring schedule gave up. */
+/* Synchronise `stream` and report whether the last assemblies completed: MAG_E_RANGE if a
+ * kernel of the tile schedule found a plan index out of range and skipped it (an internal
+ * error: the results are incomplete). The status is cleared once reported. No assembly
+ * kernel waits on another CTA or kernel. */
 int mag_mesh_check(mag_mesh *mesh, void *stream);
 /* Copy the structural pattern out (device buffers: row_ptr [num_dofs+1], col_idx [nnz]). */
 int mag_mesh_pattern(const mag_mesh *mesh, int64_t *d_row_ptr, int32_t *d_col_idx, void *stream);
@@ -314,7 +325,18 @@ int mag_pcg_solve(mag_pcg *pcg, const int64_t *d_row_ptr, const int32_t *d_col_i
  * needs mag_mesh_set_materials. Either output may be NULL. */
 int mag_element_nu(mag_mesh *mesh, const double *d_sol, double *d_nu, double *d_dnu, void *stream);
 
-/* ---- MEX-compatible entry points (host buffers, reference layout) --------- */
+/* ---- MEX-compatible entry points (host buffers, reference layout) ---------
+ * Every mag_mex_* entry point below (except mag_mex_jacobian_noalloc) keeps the
+ * device form of the last two meshes it was given, per device: P, T, Dofs and Signs
+ * converted to the library's layout and, for the sparse-returning calls, the CSR
+ * pattern. A call finds its mesh by the sizes and a 128-bit content hash of those
+ * four arrays (Tags hashed apart and reconverted when they change), so a Newton loop
+ * calling with the same mesh uploads only SolA, while an array changed in place, or
+ * a new array at a reused address, is converted afresh. The calls hold one library
+ * lock for their duration. */
+
+/* Release the device memory of the cached MEX meshes. */
+int mag_mex_cache_clear(void);
 
 /* [I,J,V,R_idx,R_val] = assemble_jacobian_kernel_mex(P,T,Dofs,Signs,Tags,SolA,
  *   Qw,CurlRef,lin,isNon,maxB,brk,coe,start,cnt,coeStart,calcJ)

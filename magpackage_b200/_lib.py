@@ -13,8 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmagasm.so")
 
 MAG_OK = 0
-SCHEDULE_TWO_PASS, SCHEDULE_L2_RING, SCHEDULE_ROW_BLOCKS, SCHEDULE_SHARED_ROW_BLOCKS = 0, 1, 2, 3
-SCHEDULE_STAGED_ROW_BLOCKS, SCHEDULE_NZ_ROW_BLOCKS = 4, 5
+SCHEDULE_TWO_PASS, SCHEDULE_ROW_BLOCKS, SCHEDULE_SHARED_ROW_BLOCKS = 0, 2, 3
+SCHEDULE_NZ_ROW_BLOCKS, SCHEDULE_TILE_BLOCKS = 5, 6
 _ERRNAMES = {-1: "MAG_E_ARG", -2: "MAG_E_RANGE", -3: "MAG_E_GEOMETRY", -4: "MAG_E_CUDA",
              -5: "MAG_E_TIMEOUT", -6: "MAG_E_NOMEM", -7: "MAG_E_UNSUPPORTED"}
 
@@ -29,8 +29,9 @@ class MeshInfo(C.Structure):
     _fields_ = [("num_nodes", C.c_int64), ("num_elements", C.c_int64), ("num_dofs", C.c_int64),
                 ("nnz", C.c_int64), ("num_incidences", C.c_int64), ("max_row_nnz", C.c_int32),
                 ("wide_positions", C.c_int32), ("signs_derived", C.c_int32), ("schedule", C.c_int32),
-                ("fused_ring_tiles", C.c_int32), ("fused_grid", C.c_int32), ("device_bytes", C.c_int64),
-                ("shared_blocks", C.c_int32), ("shared_staged", C.c_int32), ("nz_pass", C.c_int32)]
+                ("tile_blocks", C.c_int32), ("tile_colors", C.c_int32), ("device_bytes", C.c_int64),
+                ("shared_blocks", C.c_int32), ("reserved0", C.c_int32), ("nz_pass", C.c_int32),
+                ("tile_evals_per_elem", C.c_double), ("tile_plan_ms", C.c_double)]
 
 
 _vp = C.c_void_p
@@ -101,6 +102,7 @@ _PROTOS = {
                                  _int),
     "mag_mex_mass_sparse": ([_dp, _i64, _dp, _i64, _dp, _dp, _dp, _i64, _dp, _int, _dp, _i64, C.POINTER(_vp)],
                             _int),
+    "mag_mex_cache_clear": ([], _int),
     "mag_sparse_info": ([_vp, C.POINTER(_i64), C.POINTER(_i64)], _int),
     "mag_sparse_copy": ([_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _dp], _int),
     "mag_sparse_destroy": ([_vp], _int),

@@ -1,13 +1,18 @@
 // C ABI (include/magasm.h): the mesh handle, validation, and the
 // MEX-compatible entry points.
+#include <omp.h>
+
 #include <cstdarg>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <new>
+#include <vector>
 
 #include "assemble.cuh"
 #include "batch.cuh"
 #include "common.cuh"
-#include "fused.cuh"
+#include "tile.cuh"
 #include "rowblock.cuh"
 #include "internal.h"
 #include "mlp.cuh"
@@ -45,7 +50,8 @@ __global__ void k_pack_xyz(const double *__restrict__ P, int64_t nn, double4 *__
 
 // 1-based node ids stored as doubles (MEX layout) -> 0-based int32.
 __global__ void k_index_from_double(const double *__restrict__ src, int64_t n, int32_t *__restrict__ dst,
-                                    int64_t limit, int allow_zero, int *__restrict__ err) {
+                                    int64_t limit, int allow_zero, int *__restrict__ err,
+                                    int *__restrict__ maxval = nullptr) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     double v = src[i];
@@ -56,6 +62,7 @@ __global__ void k_index_from_double(const double *__restrict__ src, int64_t n, i
         k = allow_zero ? 0 : 1;
     }
     dst[i] = (int32_t)(k - 1);
+    if (maxval) atomicMax(maxval, (int)k);
 }
 
 __global__ void k_check_nodes(const int4 *__restrict__ tet, int64_t ne, int64_t nn, int *__restrict__ err) {
@@ -305,10 +312,11 @@ struct mag_mesh {
     double *d_ref = nullptr;
     MaterialStore mat;
     int has_mat = 0;
-    FusedPlan fused;
     RowBlockPlan rowblock;
     RowBlockPlan rowshared;  // 256-incidence blocks with per-block distinct-element lists
     uint8_t *second = nullptr;  // per incidence: second-contributor bits (NULL: some row has > 2)
+    TilePlan tile;              // spatial-tile blocks (default schedule)
+    int *status = nullptr;      // device word: a tile kernel skipped an out-of-range plan index
     int schedule = MAG_SCHEDULE_ROW_BLOCKS;
     int64_t bytes = 0;
 
@@ -322,11 +330,12 @@ namespace {
 
 void destroy_mesh(mag_mesh *m) {
     if (!m) return;
-    void *ptrs[] = {m->xyz, m->tet, m->dofs, m->tags, m->signbits, m->scratch, m->d_ref, m->mat.mem, m->second};
+    void *ptrs[] = {m->xyz, m->tet, m->dofs, m->tags, m->signbits, m->scratch, m->d_ref, m->mat.mem, m->second,
+                    m->status};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     free_pattern(&m->pat, nullptr);
-    free_fused_plan(&m->fused);
+    free_tile_plan(&m->tile);
     free_rowblock_plan(&m->rowblock);
     free_rowblock_plan(&m->rowshared);
     cudaDeviceSynchronize();
@@ -461,20 +470,25 @@ int mag_mesh_create(const double *d_P, int64_t Nn, const int32_t *d_T, int64_t N
         cudaGetLastError();
     }
     if (build_second_masks(m->rows(), m->pat.ninc, &m->second, s) == MAG_OK && m->second) m->bytes += m->pat.ninc;
-    if (build_rowblock_plan(m->rows(), &m->rowshared, s, kSharedBlockInc, true, nullptr, m->second) == MAG_OK &&
+    if (build_rowblock_plan(m->rows(), &m->rowshared, s, kSharedBlockInc, true, m->second) == MAG_OK &&
         m->rowshared.shared_ok) {
         m->bytes += m->rowshared.bytes;
     } else {
         free_rowblock_plan(&m->rowshared);
         cudaGetLastError();
     }
-    if (build_fused_plan(m->elems(), m->rows(), m->pat.max_row, &m->fused, s) == MAG_OK) {
-        m->bytes += m->fused.bytes;
-    } else {
-        free_fused_plan(&m->fused);
-        cudaGetLastError();
+    if (cudaMalloc(&m->status, sizeof(int)) != cudaSuccess) return fail(MAG_E_NOMEM);
+    cudaMemsetAsync(m->status, 0, sizeof(int), s);
+    {
+        const TilePlanInput ti{m->xyz, m->tet, m->dofs, m->tags, m->signbits, m->pat.row_ptr, m->pat.inc_ptr,
+                               m->pat.inc_elem, m->pat.inc_pos, Nn, Ne, num_dofs, m->pat.nnz, m->pat.ninc,
+                               m->pat.wide};
+        rc = build_tile_plan(ti, &m->tile, s);
+        if (rc != MAG_OK) return fail(rc);
+        if (m->tile.ok) m->bytes += m->tile.bytes;
     }
-    m->schedule = m->rowshared.nz_ok       ? MAG_SCHEDULE_NZ_ROW_BLOCKS
+    m->schedule = m->tile.ok               ? MAG_SCHEDULE_TILE_BLOCKS
+                  : m->rowshared.nz_ok     ? MAG_SCHEDULE_NZ_ROW_BLOCKS
                   : m->rowshared.shared_ok ? MAG_SCHEDULE_SHARED_ROW_BLOCKS
                   : m->rowblock.ok         ? MAG_SCHEDULE_ROW_BLOCKS
                                            : MAG_SCHEDULE_TWO_PASS;
@@ -506,11 +520,13 @@ int mag_mesh_get_info(const mag_mesh *m, mag_mesh_info *info) {
     info->wide_positions = m->pat.wide;
     info->signs_derived = m->signbits ? 0 : 1;
     info->schedule = m->schedule;
-    info->fused_ring_tiles = m->fused.ring_tiles;
-    info->fused_grid = m->fused.grid;
+    info->tile_blocks = m->tile.ok ? m->tile.nblocks : 0;
+    info->tile_colors = m->tile.ok ? m->tile.max_colors : 0;
+    info->tile_evals_per_elem = m->tile.ok ? m->tile.evals_per_elem : 0.0;
+    info->tile_plan_ms = m->tile.build_ms;
     info->device_bytes = m->bytes;
     info->shared_blocks = m->rowshared.shared_ok ? m->rowshared.nblocks : 0;
-    info->shared_staged = m->rowshared.staged_ok;
+    info->reserved0 = 0;
     info->nz_pass = m->rowshared.nz_ok;
     return MAG_OK;
 }
@@ -557,27 +573,27 @@ int mag_assemble_jacobian(mag_mesh *m, const double *d_sol, double *d_vals, doub
         return MAG_E_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    const bool staged = m->schedule == MAG_SCHEDULE_STAGED_ROW_BLOCKS;
-    if (m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS && m->rowshared.nz_ok && m->qp.standard_curl) {
+    if (m->schedule == MAG_SCHEDULE_TILE_BLOCKS && m->tile.ok && m->qp.standard_curl) {
+        MAG_TRY(launch_tile_jacobian(m->tile, m->elems(), d_sol, m->qp, m->mat.mp, calc_j, calc_j ? d_vals : nullptr,
+                                     d_res, m->status, s));
+        return finish(s);
+    }
+    if ((m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_TILE_BLOCKS) &&
+        m->rowshared.nz_ok && m->qp.standard_curl) {
         MAG_TRY(launch_rowblock_nz_jacobian(m->rowshared, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp, calc_j,
                                             calc_j ? d_vals : nullptr, d_res, s));
         return finish(s);
     }
-    if ((m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || staged || m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS) &&
-        m->rowshared.shared_ok && m->qp.standard_curl) {
+    const bool rowsched = m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_TILE_BLOCKS;
+    if ((m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || rowsched) && m->rowshared.shared_ok &&
+        m->qp.standard_curl) {
         MAG_TRY(launch_rowblock_shared_jacobian(m->rowshared, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp,
-                                                calc_j, calc_j ? d_vals : nullptr, d_res, s, staged));
+                                                calc_j, calc_j ? d_vals : nullptr, d_res, s));
         return finish(s);
     }
-    if (m->schedule == MAG_SCHEDULE_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || staged ||
-        m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS) {
+    if (m->schedule == MAG_SCHEDULE_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_SHARED_ROW_BLOCKS || rowsched) {
         MAG_TRY(launch_rowblock_jacobian(m->rowblock, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp, calc_j,
                                          calc_j ? d_vals : nullptr, d_res, s));
-        return finish(s);
-    }
-    if (m->schedule == MAG_SCHEDULE_L2_RING) {
-        MAG_TRY(launch_fused_jacobian(m->fused, m->elems(), m->rows(), d_sol, m->qp, m->mat.mp, calc_j,
-                                      calc_j ? d_vals : nullptr, d_res, s));
         return finish(s);
     }
     MAG_TRY(launch_jacobian_elems(m->elems(), d_sol, m->qp, m->mat.mp, calc_j, m->scratch, s));
@@ -592,7 +608,12 @@ int mag_assemble_stiffness(mag_mesh *m, const double *d_nu, double *d_vals, void
         return MAG_E_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    if (m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS && m->rowshared.nz_ok && m->qp.standard_curl) {
+    if (m->schedule == MAG_SCHEDULE_TILE_BLOCKS && m->tile.ok && m->qp.standard_curl) {
+        MAG_TRY(launch_tile_stiffness(m->tile, m->elems(), d_nu, m->qp, d_vals, m->status, s));
+        return finish(s);
+    }
+    if ((m->schedule == MAG_SCHEDULE_NZ_ROW_BLOCKS || m->schedule == MAG_SCHEDULE_TILE_BLOCKS) &&
+        m->rowshared.nz_ok && m->qp.standard_curl) {
         MAG_TRY(launch_rowblock_nz_stiffness(m->rowshared, m->elems(), m->rows(), d_nu, m->qp, d_vals, s));
         return finish(s);
     }
@@ -734,25 +755,11 @@ int mag_mesh_set_option(mag_mesh *m, int option, int64_t value) {
         return MAG_E_ARG;
     }
     if (option == MAG_OPTION_SCHEDULE) {
-        if (value == MAG_SCHEDULE_STAGED_ROW_BLOCKS && m->rowshared.shared_ok && !m->rowshared.staged_ok) {
-            // the staging tables are built on first request (blocks re-split to their capacity)
-            RowBlockPlan staged{};
-            const ElemData ed = m->elems();
-            if (build_rowblock_plan(m->rows(), &staged, nullptr, kSharedBlockInc, true, &ed, m->second) == MAG_OK &&
-                staged.shared_ok && staged.staged_ok) {
-                m->bytes += staged.bytes - m->rowshared.bytes;
-                free_rowblock_plan(&m->rowshared);
-                m->rowshared = staged;
-            } else {
-                free_rowblock_plan(&staged);
-                cudaGetLastError();
-            }
-        }
-        if ((value == MAG_SCHEDULE_L2_RING && !m->fused.ok) ||
+        if (value == MAG_SCHEDULE_RETIRED_1 || value == MAG_SCHEDULE_RETIRED_4 ||
             (value == MAG_SCHEDULE_ROW_BLOCKS && !m->rowblock.ok) ||
             (value == MAG_SCHEDULE_SHARED_ROW_BLOCKS && !m->rowshared.shared_ok) ||
-            (value == MAG_SCHEDULE_STAGED_ROW_BLOCKS && !m->rowshared.staged_ok) ||
-            (value == MAG_SCHEDULE_NZ_ROW_BLOCKS && !m->rowshared.nz_ok) || value < 0 || value > 5) {
+            (value == MAG_SCHEDULE_NZ_ROW_BLOCKS && !m->rowshared.nz_ok) ||
+            (value == MAG_SCHEDULE_TILE_BLOCKS && !m->tile.ok) || value < 0 || value > 6) {
             set_error("assembly schedule %lld is not available for this mesh", (long long)value);
             return MAG_E_UNSUPPORTED;
         }
@@ -769,9 +776,17 @@ int mag_mesh_check(mag_mesh *m, void *stream) {
         return MAG_E_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    MAG_TRY(fused_status(m->fused, s));
+    int h = 0;
+    MAG_CUDA_TRY(cudaMemcpyAsync(&h, m->status, sizeof(int), cudaMemcpyDeviceToHost, s));
     MAG_CUDA_TRY(cudaStreamSynchronize(s));
     MAG_CUDA_TRY(cudaGetLastError());
+    if (h) {
+        MAG_CUDA_TRY(cudaMemsetAsync(m->status, 0, sizeof(int), s));
+        MAG_CUDA_TRY(cudaStreamSynchronize(s));
+        set_error("tile schedule: a plan index was out of range and was skipped (internal error); the last "
+                  "assemblies are incomplete");
+        return MAG_E_RANGE;
+    }
     return MAG_OK;
 }
 
@@ -1193,63 +1208,208 @@ int mag_pcg_solve(mag_pcg *p, const int64_t *rp, const int32_t *ci, const double
 
 namespace {
 
+// A mesh given in the reference's MEX layout, converted to the device layout. The MEX
+// entry points keep the last kMexCacheEntries of them (per device), keyed by the sizes
+// and a content hash of P, T, Dofs and Signs, so that the Newton loop's calls with the
+// same mesh (Assembler.m:199-202 every iteration and line-search step) neither upload
+// nor convert nor plan it again; an array changed in place, or a new array at a reused
+// address, hashes differently and is converted afresh. Tags are hashed separately and
+// reconverted when they change.
 struct MexMesh {
-    Dev xyz, tet, dofs, tags, signs, P, Td, Dd, Sd, Gd, scratch;
+    Dev xyz, tet, dofs, tags, signs, scratch;
     ElemData ed{};
-    explicit MexMesh(cudaStream_t s)
-        : xyz(s), tet(s), dofs(s), tags(s), signs(s), P(s), Td(s), Dd(s), Sd(s), Gd(s), scratch(s) {}
+    int dev = -1;
+    int64_t Nn = 0, Ne = 0;
+    uint64_t h0 = 0, h1 = 0;       // content hash of P, T, Dofs, Signs
+    int has_tags = 0;
+    uint64_t t0 = 0, t1 = 0;       // content hash of Tags
+    int max_tag = 0;
+    int max_dof = 0;               // largest 1-based dof (0 = missing) the element arrays use
+    PatternBuffers pat;            // CSR pattern of the sparse-returning entry points
+    int64_t pat_ndof = -1;
+    uint64_t stamp = 0;
+    explicit MexMesh(cudaStream_t s) : xyz(s), tet(s), dofs(s), tags(s), signs(s), scratch(s) {}
+    ~MexMesh() { free_pattern(&pat, nullptr); }
 };
 
-// Upload the reference's double arrays and convert them to the device layout.
-int mex_upload(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
-               const double *Signs, const double *Tags, int64_t dof_limit, MexMesh &mm, int *max_tag,
-               cudaStream_t s) {
-    if (!P || !T || !Dofs || !Signs || Nn <= 0 || Ne <= 0) {
-        set_error("mex: bad arguments");
-        return MAG_E_ARG;
+constexpr size_t kMexCacheEntries = 2;
+std::mutex g_mex_mu;  // held for the whole of every MEX entry point (the cached scratch is shared)
+std::vector<std::unique_ptr<MexMesh>> g_mex_cache;
+uint64_t g_mex_clock = 0;
+
+inline uint64_t mix64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xFF51AFD7ED558CCDull;
+    x ^= x >> 33;
+    x *= 0xC4CEB9FE1A85EC53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+// Two-lane 64-bit content hash of a host array, folded into (h0, h1); 1 MiB chunks
+// are hashed on the host threads and combined in order.
+void hash_host(const void *data, size_t bytes, uint64_t &h0, uint64_t &h1) {
+    constexpr size_t C = size_t(1) << 20;
+    const size_t n = (bytes + C - 1) / C;
+    std::vector<uint64_t> a(n), b(n);
+    const unsigned char *c = static_cast<const unsigned char *>(data);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < (int64_t)n; k++) {
+        const size_t o = (size_t)k * C, len = bytes - o < C ? bytes - o : C;
+        uint64_t x = 0x243F6A8885A308D3ull + (uint64_t)k, y = 0x13198A2E03707344ull ^ (uint64_t)k;
+        size_t i = 0;
+        for (; i + 8 <= len; i += 8) {
+            uint64_t v;
+            std::memcpy(&v, c + o + i, 8);
+            x = (x ^ v) * 0x9E3779B97F4A7C15ull;
+            x ^= x >> 29;
+            y = (y + v) * 0xC2B2AE3D27D4EB4Full;
+            y ^= y >> 31;
+        }
+        for (; i < len; i++) {
+            x = (x ^ c[o + i]) * 0x9E3779B97F4A7C15ull;
+            y = (y + c[o + i]) * 0xC2B2AE3D27D4EB4Full;
+        }
+        a[k] = mix64(x);
+        b[k] = mix64(y ^ len);
     }
-    Dev err(s), mx(s);
+    for (size_t k = 0; k < n; k++) {
+        h0 = mix64(h0 ^ a[k]) + k;
+        h1 = mix64(h1 + b[k]) ^ k;
+    }
+    h0 = mix64(h0 ^ bytes);
+    h1 = mix64(h1 + bytes);
+}
+
+// Upload the reference's double arrays (P, T, Dofs, Signs) and convert them.
+int mex_convert(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+                const double *Signs, MexMesh &mm, cudaStream_t s) {
+    Dev err(s), mxd(s), Pd(s), Td(s), Dd(s), Sd(s);
     MAG_CUDA_TRY(err.alloc(4));
-    MAG_CUDA_TRY(mx.alloc(4));
+    MAG_CUDA_TRY(mxd.alloc(4));
     MAG_CUDA_TRY(cudaMemsetAsync(err.p, 0, 4, s));
-    MAG_CUDA_TRY(cudaMemsetAsync(mx.p, 0, 4, s));
-    MAG_CUDA_TRY(mm.P.alloc(Nn * 24));
-    MAG_CUDA_TRY(mm.Td.alloc(Ne * 32));
-    MAG_CUDA_TRY(mm.Dd.alloc(Ne * 48));
-    MAG_CUDA_TRY(mm.Sd.alloc(Ne * 48));
+    MAG_CUDA_TRY(cudaMemsetAsync(mxd.p, 0, 4, s));
+    MAG_CUDA_TRY(Pd.alloc(Nn * 24));
+    MAG_CUDA_TRY(Td.alloc(Ne * 32));
+    MAG_CUDA_TRY(Dd.alloc(Ne * 48));
+    MAG_CUDA_TRY(Sd.alloc(Ne * 48));
     MAG_CUDA_TRY(mm.xyz.alloc(Nn * sizeof(double4)));
     MAG_CUDA_TRY(mm.tet.alloc(Ne * 16));
     MAG_CUDA_TRY(mm.dofs.alloc(Ne * 24));
     MAG_CUDA_TRY(mm.tags.alloc(Ne));
     MAG_CUDA_TRY(mm.signs.alloc(Ne));
-    MAG_CUDA_TRY(cudaMemcpyAsync(mm.P.p, P, Nn * 24, cudaMemcpyHostToDevice, s));
-    MAG_CUDA_TRY(cudaMemcpyAsync(mm.Td.p, T, Ne * 32, cudaMemcpyHostToDevice, s));
-    MAG_CUDA_TRY(cudaMemcpyAsync(mm.Dd.p, Dofs, Ne * 48, cudaMemcpyHostToDevice, s));
-    MAG_CUDA_TRY(cudaMemcpyAsync(mm.Sd.p, Signs, Ne * 48, cudaMemcpyHostToDevice, s));
-    k_pack_xyz<<<grid(Nn), kB, 0, s>>>(mm.P.as<double>(), Nn, mm.xyz.as<double4>(), err.as<int>());
-    k_index_from_double<<<grid(4 * Ne), kB, 0, s>>>(mm.Td.as<double>(), 4 * Ne, mm.tet.as<int32_t>(), Nn, 0,
+    MAG_CUDA_TRY(cudaMemcpyAsync(Pd.p, P, Nn * 24, cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(Td.p, T, Ne * 32, cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(Dd.p, Dofs, Ne * 48, cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(Sd.p, Signs, Ne * 48, cudaMemcpyHostToDevice, s));
+    k_pack_xyz<<<grid(Nn), kB, 0, s>>>(Pd.as<double>(), Nn, mm.xyz.as<double4>(), err.as<int>());
+    k_index_from_double<<<grid(4 * Ne), kB, 0, s>>>(Td.as<double>(), 4 * Ne, mm.tet.as<int32_t>(), Nn, 0,
                                                     err.as<int>());
-    k_index_from_double<<<grid(6 * Ne), kB, 0, s>>>(mm.Dd.as<double>(), 6 * Ne, mm.dofs.as<int32_t>(),
-                                                    dof_limit, 1, err.as<int>());
-    k_pack_signs_f64<<<grid(Ne), kB, 0, s>>>(mm.Sd.as<double>(), Ne, mm.signs.as<uint8_t>(), err.as<int>());
-    if (Tags) {
-        MAG_CUDA_TRY(mm.Gd.alloc(Ne * 8));
-        MAG_CUDA_TRY(cudaMemcpyAsync(mm.Gd.p, Tags, Ne * 8, cudaMemcpyHostToDevice, s));
-        k_pack_tags_f64<<<grid(Ne), kB, 0, s>>>(mm.Gd.as<double>(), Ne, mm.tags.as<uint8_t>(), mx.as<int>(),
-                                                err.as<int>());
-    } else {
-        MAG_CUDA_TRY(cudaMemsetAsync(mm.tags.p, 1, Ne, s));
-    }
+    k_index_from_double<<<grid(6 * Ne), kB, 0, s>>>(Dd.as<double>(), 6 * Ne, mm.dofs.as<int32_t>(),
+                                                    (int64_t)INT32_MAX, 1, err.as<int>(), mxd.as<int>());
+    k_pack_signs_f64<<<grid(Ne), kB, 0, s>>>(Sd.as<double>(), Ne, mm.signs.as<uint8_t>(), err.as<int>());
+    MAG_CUDA_TRY(cudaMemsetAsync(mm.tags.p, 1, Ne, s));
     int h = 0;
     MAG_TRY(sync_flag(err.as<int>(), s, &h));
     if (h) {
-        set_error("mex: index, sign or tag out of range (nodes 1..Nn, dofs 0..numel(SolA), signs +-1, tags 1..255)");
+        set_error("mex: index or sign out of range (nodes 1..Nn, dofs 0..numel(SolA), signs +-1)");
         return MAG_E_RANGE;
     }
-    MAG_TRY(sync_flag(mx.as<int>(), s, max_tag));
+    MAG_TRY(sync_flag(mxd.as<int>(), s, &mm.max_dof));
     mm.ed = ElemData{mm.xyz.as<double4>(), mm.tet.as<int4>(), mm.dofs.as<int32_t>(),
                      mm.tags.as<uint8_t>(), mm.signs.as<uint8_t>(), Ne};
     MAG_CUDA_TRY(mm.scratch.alloc((size_t)Ne * kScratchPerElem * 8));
+    return MAG_OK;
+}
+
+int mex_set_tags(MexMesh &mm, const double *Tags, cudaStream_t s) {
+    Dev err(s), mx(s), Gd(s);
+    MAG_CUDA_TRY(err.alloc(4));
+    MAG_CUDA_TRY(mx.alloc(4));
+    MAG_CUDA_TRY(Gd.alloc(mm.Ne * 8));
+    MAG_CUDA_TRY(cudaMemsetAsync(err.p, 0, 4, s));
+    MAG_CUDA_TRY(cudaMemsetAsync(mx.p, 0, 4, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(Gd.p, Tags, mm.Ne * 8, cudaMemcpyHostToDevice, s));
+    k_pack_tags_f64<<<grid(mm.Ne), kB, 0, s>>>(Gd.as<double>(), mm.Ne, mm.tags.as<uint8_t>(), mx.as<int>(),
+                                               err.as<int>());
+    int h = 0;
+    MAG_TRY(sync_flag(err.as<int>(), s, &h));
+    mm.has_tags = 0;
+    if (h) {
+        set_error("mex: tag out of range (tags 1..255)");
+        return MAG_E_RANGE;
+    }
+    MAG_TRY(sync_flag(mx.as<int>(), s, &mm.max_tag));
+    mm.has_tags = 1;
+    return MAG_OK;
+}
+
+// The device mesh for these MEX arrays: from the cache, or converted and cached.
+// dof_limit: every dof must be <= it (numel(SolA) for the Jacobian); Tags may be NULL.
+// The caller holds g_mex_mu.
+int mex_mesh(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
+             const double *Signs, const double *Tags, int64_t dof_limit, MexMesh **out, int *max_tag,
+             cudaStream_t s) {
+    *out = nullptr;
+    if (!P || !T || !Dofs || !Signs || Nn <= 0 || Ne <= 0) {
+        set_error("mex: bad arguments");
+        return MAG_E_ARG;
+    }
+    int dev = 0;
+    MAG_CUDA_TRY(cudaGetDevice(&dev));
+    uint64_t h0 = 0x6A09E667F3BCC908ull, h1 = 0xBB67AE8584CAA73Bull;
+    hash_host(P, (size_t)Nn * 24, h0, h1);
+    hash_host(T, (size_t)Ne * 32, h0, h1);
+    hash_host(Dofs, (size_t)Ne * 48, h0, h1);
+    hash_host(Signs, (size_t)Ne * 48, h0, h1);
+    MexMesh *mm = nullptr;
+    for (auto &e : g_mex_cache)
+        if (e->dev == dev && e->Nn == Nn && e->Ne == Ne && e->h0 == h0 && e->h1 == h1) mm = e.get();
+    if (!mm) {
+        std::unique_ptr<MexMesh> fresh(new (std::nothrow) MexMesh(s));
+        if (!fresh) return MAG_E_NOMEM;
+        if (g_mex_cache.size() >= kMexCacheEntries) {  // evict the least recently used
+            size_t lru = 0;
+            for (size_t i = 1; i < g_mex_cache.size(); i++)
+                if (g_mex_cache[i]->stamp < g_mex_cache[lru]->stamp) lru = i;
+            g_mex_cache.erase(g_mex_cache.begin() + (long)lru);
+        }
+        MAG_TRY(mex_convert(P, Nn, T, Ne, Dofs, Signs, *fresh, s));
+        fresh->dev = dev;
+        fresh->Nn = Nn;
+        fresh->Ne = Ne;
+        fresh->h0 = h0;
+        fresh->h1 = h1;
+        mm = fresh.get();
+        g_mex_cache.push_back(std::move(fresh));
+    }
+    mm->stamp = ++g_mex_clock;
+    if (Tags) {
+        uint64_t t0 = 0x3C6EF372FE94F82Bull, t1 = 0xA54FF53A5F1D36F1ull;
+        hash_host(Tags, (size_t)Ne * 8, t0, t1);
+        if (!mm->has_tags || mm->t0 != t0 || mm->t1 != t1) {
+            MAG_TRY(mex_set_tags(*mm, Tags, s));
+            mm->t0 = t0;
+            mm->t1 = t1;
+        }
+    }
+    if (mm->max_dof > dof_limit) {
+        set_error("mex: dof %d out of range (dofs 0..%lld)", mm->max_dof, (long long)dof_limit);
+        return MAG_E_RANGE;
+    }
+    *max_tag = Tags ? mm->max_tag : 0;
+    *out = mm;
+    return MAG_OK;
+}
+
+// The CSR pattern of a cached MEX mesh with ndof rows (built on first use).
+int mex_pattern(MexMesh &mm, int64_t ndof, cudaStream_t s) {
+    if (mm.pat_ndof == ndof) return MAG_OK;
+    free_pattern(&mm.pat, s);
+    mm.pat = PatternBuffers{};
+    mm.pat_ndof = -1;
+    MAG_TRY(build_pattern(mm.dofs.as<int32_t>(), mm.Ne, ndof, &mm.pat, s));
+    mm.pat_ndof = ndof;
     return MAG_OK;
 }
 
@@ -1277,11 +1437,11 @@ int mex_download(MexMesh &mm, int64_t Ne, int calcj, double *I, double *J, doubl
 // The Jacobian element phase of the MEX entry points: upload, materials, quadrature,
 // element blocks and residual entries into mm.scratch.
 struct MexJacobian {
-    MexMesh mm;
+    MexMesh *mm = nullptr;
     MaterialStore ms{};
     double *q = nullptr;
     Dev sol;
-    explicit MexJacobian(cudaStream_t s) : mm(s), sol(s) {}
+    explicit MexJacobian(cudaStream_t s) : sol(s) {}
     ~MexJacobian() {
         if (ms.mem) cudaFree(ms.mem);
         if (q) cudaFree(q);
@@ -1292,7 +1452,7 @@ struct MexJacobian {
             const double *brk, int nbrk, const double *coe, int ncoe, const double *start, const double *cnt,
             const double *coeStart, int calc_j, cudaStream_t s) {
         int max_tag = 0;
-        MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, Tags, Ndof, mm, &max_tag, s));
+        MAG_TRY(mex_mesh(P, Nn, T, Ne, Dofs, Signs, Tags, Ndof, &mm, &max_tag, s));
         MAG_TRY(upload_materials(lin, isNon, maxB, nmat, brk, nbrk, coe, ncoe, start, cnt, coeStart, &ms, s));
         if (nmat < max_tag) {
             set_error("mag_mex_jacobian: tag %d has no material entry", max_tag);
@@ -1304,11 +1464,18 @@ struct MexJacobian {
         // dofs must index SolA
         MAG_CUDA_TRY(sol.alloc(Ndof * 8));
         MAG_CUDA_TRY(cudaMemcpyAsync(sol.p, SolA, Ndof * 8, cudaMemcpyHostToDevice, s));
-        return launch_jacobian_elems(mm.ed, sol.as<double>(), qp, ms.mp, calc_j, mm.scratch.as<double>(), s);
+        return launch_jacobian_elems(mm->ed, sol.as<double>(), qp, ms.mp, calc_j, mm->scratch.as<double>(), s);
     }
 };
 
 }  // namespace
+
+int mag_mex_cache_clear(void) {
+    std::lock_guard<std::mutex> lk(g_mex_mu);
+    g_mex_cache.clear();
+    MAG_CUDA_TRY(cudaDeviceSynchronize());
+    return MAG_OK;
+}
 
 int mag_mex_jacobian(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
                      const double *Signs, const double *Tags, const double *SolA, int64_t Ndof,
@@ -1323,10 +1490,11 @@ int mag_mex_jacobian(const double *P, int64_t Nn, const double *T, int64_t Ne, c
         set_error("mag_mex_jacobian: bad arguments");
         return MAG_E_ARG;
     }
+    std::lock_guard<std::mutex> lk(g_mex_mu);
     MexJacobian mj(s);
     MAG_TRY(mj.run(P, Nn, T, Ne, Dofs, Signs, Tags, SolA, Ndof, Qw, nq, CurlRef, lin, isNon, maxB, nmat, brk,
                    nbrk, coe, ncoe, start, cnt, coeStart, calc_j, s));
-    return mex_download(mj.mm, Ne, calc_j, I, J, V, R_idx, R_val, s);
+    return mex_download(*mj.mm, Ne, calc_j, I, J, V, R_idx, R_val, s);
 }
 
 int mag_mex_curl_curl(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
@@ -1338,9 +1506,11 @@ int mag_mex_curl_curl(const double *P, int64_t Nn, const double *T, int64_t Ne, 
         set_error("mag_mex_curl_curl: bad arguments");
         return MAG_E_ARG;
     }
-    MexMesh mm(s);
+    std::lock_guard<std::mutex> lk(g_mex_mu);
+    MexMesh *mmp = nullptr;
     int max_tag = 0;
-    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, (int64_t)1 << 31, mm, &max_tag, s));
+    MAG_TRY(mex_mesh(P, Nn, T, Ne, Dofs, Signs, nullptr, (int64_t)1 << 31, &mmp, &max_tag, s));
+    MexMesh &mm = *mmp;
     QuadParams qp{};
     double *dq = nullptr;
     MAG_TRY(make_quad(Qw, nq, CurlRef, CurlRef, &qp, &dq, s));
@@ -1362,9 +1532,11 @@ int mag_mex_mass(const double *P, int64_t Nn, const double *T, int64_t Ne, const
         set_error("mag_mex_mass: bad arguments");
         return MAG_E_ARG;
     }
-    MexMesh mm(s);
+    std::lock_guard<std::mutex> lk(g_mex_mu);
+    MexMesh *mmp = nullptr;
     int max_tag = 0;
-    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, (int64_t)1 << 31, mm, &max_tag, s));
+    MAG_TRY(mex_mesh(P, Nn, T, Ne, Dofs, Signs, nullptr, (int64_t)1 << 31, &mmp, &max_tag, s));
+    MexMesh &mm = *mmp;
     QuadParams qp{};
     double *dq = nullptr;
     MAG_TRY(make_quad(Qw, nq, ValRef, ValRef, &qp, &dq, s));
@@ -1394,9 +1566,11 @@ int mag_mex_source(const double *P, int64_t Nn, const double *T, int64_t Ne, con
         set_error("mag_mex_source: bad arguments");
         return MAG_E_ARG;
     }
-    MexMesh mm(s);
+    std::lock_guard<std::mutex> lk(g_mex_mu);
+    MexMesh *mmp = nullptr;
     int max_tag = 0;
-    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, (int64_t)1 << 31, mm, &max_tag, s));
+    MAG_TRY(mex_mesh(P, Nn, T, Ne, Dofs, Signs, nullptr, (int64_t)1 << 31, &mmp, &max_tag, s));
+    MexMesh &mm = *mmp;
     QuadParams qp{};
     double *dq = nullptr;
     MAG_TRY(make_quad(Qw, nq, ValRef, ValRef, &qp, &dq, s));
@@ -1426,9 +1600,11 @@ int mag_mex_winding(const double *P, int64_t Nn, const double *T, int64_t Ne, co
         set_error("mag_mex_winding: bad arguments");
         return MAG_E_ARG;
     }
-    MexMesh mm(s);
+    std::lock_guard<std::mutex> lk(g_mex_mu);
+    MexMesh *mmp = nullptr;
     int max_tag = 0;
-    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, Tags, (int64_t)1 << 31, mm, &max_tag, s));
+    MAG_TRY(mex_mesh(P, Nn, T, Ne, Dofs, Signs, Tags, (int64_t)1 << 31, &mmp, &max_tag, s));
+    MexMesh &mm = *mmp;
     QuadParams qp{};
     double *dq = nullptr;
     MAG_TRY(make_quad(Qw, nq, ValRef, ValRef, &qp, &dq, s));
@@ -1525,12 +1701,8 @@ int empty_sparse(int64_t ndof, mag_sparse **out) {
 // (I > 0) & (J > 0) filter of Assembler.m:37,52,71,205 drops them.
 int mex_to_sparse(MexMesh &mm, int64_t Ne, int64_t ndof, bool with_matrix, double *h_res, mag_sparse **out,
                   cudaStream_t s) {
-    PatternBuffers pat;
-    struct PatGuard {
-        PatternBuffers &p;
-        ~PatGuard() { free_pattern(&p, nullptr); }
-    } pg{pat};
-    MAG_TRY(build_pattern(mm.dofs.as<int32_t>(), Ne, ndof, &pat, s));
+    MAG_TRY(mex_pattern(mm, ndof, s));
+    const PatternBuffers &pat = mm.pat;
     const RowPlan rows{pat.row_ptr, pat.inc_ptr, pat.inc_elem, pat.inc_pos, ndof, pat.wide};
     Dev vals(s), rp64(s), res(s);
     if (with_matrix) {
@@ -1591,10 +1763,11 @@ int mag_mex_jacobian_sparse(const double *P, int64_t Nn, const double *T, int64_
         set_error("mag_mex_jacobian_sparse: bad arguments");
         return MAG_E_ARG;
     }
+    std::lock_guard<std::mutex> lk(g_mex_mu);
     MexJacobian mj(s);
     MAG_TRY(mj.run(P, Nn, T, Ne, Dofs, Signs, Tags, SolA, Ndof, Qw, nq, CurlRef, lin, isNon, maxB, nmat, brk,
                    nbrk, coe, ncoe, start, cnt, coeStart, calc_j, s));
-    return mex_to_sparse(mj.mm, Ne, Ndof, calc_j != 0, R, J_out, s);
+    return mex_to_sparse(*mj.mm, Ne, Ndof, calc_j != 0, R, J_out, s);
 }
 
 int mag_mex_curl_curl_sparse(const double *P, int64_t Nn, const double *T, int64_t Ne, const double *Dofs,
@@ -1607,9 +1780,11 @@ int mag_mex_curl_curl_sparse(const double *P, int64_t Nn, const double *T, int64
         return MAG_E_ARG;
     }
     if (Ne == 0) return empty_sparse(Ndof, out);
-    MexMesh mm(s);
+    std::lock_guard<std::mutex> lk(g_mex_mu);
+    MexMesh *mmp = nullptr;
     int max_tag = 0;
-    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, Ndof, mm, &max_tag, s));
+    MAG_TRY(mex_mesh(P, Nn, T, Ne, Dofs, Signs, nullptr, Ndof, &mmp, &max_tag, s));
+    MexMesh &mm = *mmp;
     QuadParams qp{};
     double *dq = nullptr;
     MAG_TRY(make_quad(Qw, nq, CurlRef, CurlRef, &qp, &dq, s));
@@ -1632,9 +1807,11 @@ int mag_mex_mass_sparse(const double *P, int64_t Nn, const double *T, int64_t Ne
         return MAG_E_ARG;
     }
     if (Ne == 0) return empty_sparse(Ndof, out);
-    MexMesh mm(s);
+    std::lock_guard<std::mutex> lk(g_mex_mu);
+    MexMesh *mmp = nullptr;
     int max_tag = 0;
-    MAG_TRY(mex_upload(P, Nn, T, Ne, Dofs, Signs, nullptr, Ndof, mm, &max_tag, s));
+    MAG_TRY(mex_mesh(P, Nn, T, Ne, Dofs, Signs, nullptr, Ndof, &mmp, &max_tag, s));
+    MexMesh &mm = *mmp;
     QuadParams qp{};
     double *dq = nullptr;
     MAG_TRY(make_quad(Qw, nq, ValRef, ValRef, &qp, &dq, s));

@@ -315,139 +315,6 @@ __global__ void __launch_bounds__(BI) k_block_elems(RowPlan rp, const int32_t *_
     }
 }
 
-// Sort n (<= N) keys in shared memory with the block's threads (bitonic network).
-template <int N>
-__device__ void block_sort(uint32_t *key) {
-    for (int k = 2; k <= N; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < N; i += blockDim.x) {
-                const int p = i ^ j;
-                if (p > i) {
-                    uint32_t x = key[i], y = key[p];
-                    if ((x > y) == ((i & k) == 0)) {
-                        key[i] = y;
-                        key[p] = x;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
-// Compact the distinct keys (below 0xFFFFFFFF) of a sorted array in place; returns the count.
-template <int N>
-__device__ int block_unique(uint32_t *key, int *part) {
-    constexpr int PER = N / kBlockInc;
-    const int t = threadIdx.x;
-    uint32_t v[PER];
-    int f = 0;
-#pragma unroll
-    for (int q = 0; q < PER; q++) {
-        const int i = t * PER + q;
-        v[q] = key[i];
-        if (v[q] != 0xFFFFFFFFu && (i == 0 || key[i - 1] != v[q])) f++;
-    }
-    part[t] = f;
-    __syncthreads();
-    for (int off = 1; off < kBlockInc; off <<= 1) {
-        int x = t >= off ? part[t - off] : 0;
-        __syncthreads();
-        part[t] += x;
-        __syncthreads();
-    }
-    int pos = part[t] - f;
-    const int total = part[kBlockInc - 1];
-    __syncthreads();
-    bool first[PER];
-#pragma unroll
-    for (int q = 0; q < PER; q++) {
-        const int i = t * PER + q;
-        first[q] = v[q] != 0xFFFFFFFFu && (i == 0 || key[i - 1] != v[q]);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PER; q++)
-        if (first[q]) key[pos++] = v[q];
-    __syncthreads();
-    return total;
-}
-
-__device__ __forceinline__ int find_key(const uint32_t *key, int n, uint32_t x) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (key[mid] < x) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
-// Per block: its distinct nodes and edge dofs and, per distinct element, the record
-// (4 local node indices | 6 local edge indices, 0x3FF = no dof | tag | sign bits).
-// mode 0 writes the counts; mode 1 writes the lists at the offsets.
-__global__ void __launch_bounds__(kBlockInc) k_block_stage(ElemData m, const int32_t *__restrict__ blk_nelem,
-                                                           const int32_t *__restrict__ blk_k0,
-                                                           const int32_t *__restrict__ blk_elem, int mode,
-                                                           int32_t *__restrict__ cnt, const int32_t *__restrict__ off,
-                                                           int32_t *__restrict__ node_out,
-                                                           int32_t *__restrict__ edge_out,
-                                                           uint4 *__restrict__ erec_out) {
-    constexpr int NK = 1024, DK = 2048;  // >= 4 and 6 keys per element for kMaxBlockElems elements
-    static_assert(NK >= 4 * kMaxBlockElems && DK >= 6 * kMaxBlockElems, "staging key capacity");
-    __shared__ uint32_t nkey[NK], dkey[DK];
-    __shared__ int part[kBlockInc];
-    const int b = blockIdx.x, t = threadIdx.x;
-    const int nel = blk_nelem[b], k0 = blk_k0[b];
-    for (int i = t; i < NK; i += kBlockInc) nkey[i] = 0xFFFFFFFFu;
-    for (int i = t; i < DK; i += kBlockInc) dkey[i] = 0xFFFFFFFFu;
-    __syncthreads();
-    for (int u = t; u < nel; u += kBlockInc) {
-        const int64_t e = blk_elem[k0 + u];
-        const int4 tt = m.tet[e];
-        nkey[4 * u] = (uint32_t)tt.x;
-        nkey[4 * u + 1] = (uint32_t)tt.y;
-        nkey[4 * u + 2] = (uint32_t)tt.z;
-        nkey[4 * u + 3] = (uint32_t)tt.w;
-        int d[6];
-        load_dofs(m.dofs, e, d);
-#pragma unroll
-        for (int i = 0; i < 6; i++) dkey[6 * u + i] = d[i] >= 0 ? (uint32_t)d[i] : 0xFFFFFFFFu;
-    }
-    __syncthreads();
-    block_sort<NK>(nkey);
-    block_sort<DK>(dkey);
-    const int nn = block_unique<NK>(nkey, part);
-    const int nd = block_unique<DK>(dkey, part);
-    if (mode == 0) {
-        if (t == 0) {
-            cnt[2 * b] = nn;
-            cnt[2 * b + 1] = nd;
-        }
-        return;
-    }
-    const int noff = off[3 * b], doff = off[3 * b + 1], eoff = off[3 * b + 2];
-    for (int i = t; i < nn; i += kBlockInc) node_out[noff + i] = (int32_t)nkey[i];
-    for (int i = t; i < nd; i += kBlockInc) edge_out[doff + i] = (int32_t)dkey[i];
-    for (int u = t; u < nel; u += kBlockInc) {
-        const int64_t e = blk_elem[k0 + u];
-        const int4 tt = m.tet[e];
-        int d[6];
-        load_dofs(m.dofs, e, d);
-        const unsigned sb = m.signbits ? m.signbits[e] : derived_signs(tt);
-        unsigned li[6];
-#pragma unroll
-        for (int i = 0; i < 6; i++) li[i] = d[i] >= 0 ? (unsigned)find_key(dkey, nd, (uint32_t)d[i]) : 0x3FFu;
-        uint4 r;
-        r.x = (unsigned)find_key(nkey, nn, (uint32_t)tt.x) | (unsigned)find_key(nkey, nn, (uint32_t)tt.y) << 8 |
-              (unsigned)find_key(nkey, nn, (uint32_t)tt.z) << 16 | (unsigned)find_key(nkey, nn, (uint32_t)tt.w) << 24;
-        r.y = li[0] | li[1] << 10 | li[2] << 20;
-        r.z = li[3] | li[4] << 10 | li[5] << 20;
-        r.w = (unsigned)m.tags[e] | sb << 8;
-        erec_out[eoff + u] = r;
-    }
-}
-
 constexpr int kSv2 = 7;  // shared-memory stride (doubles) of one incidence's values
 
 // One distinct element of a block, evaluated once: what every row of the element needs.
@@ -480,20 +347,12 @@ struct SharedLayout {
 // threads (rows ~16 nonzeros apart) adding at the same in-row position hit different banks.
 __device__ __forceinline__ int skew(int i) { return i + (i >> 4); }
 
-// Staging tables of a block (STAGED kernels): node ids, edge dofs, element records.
-struct StageArgs {
-    const int32_t *cnt, *off, *node, *edge;
-    const uint4 *erec;
-};
-
-template <int BI, int MAXE, int MINB, bool CALCJ, bool Q4, bool WIDE, bool STAGED>
+template <int BI, int MAXE, int MINB, bool CALCJ, bool Q4, bool WIDE>
 __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const int32_t *__restrict__ blk_nelem,
                                                               const int32_t *__restrict__ blk_k0,
                                                               const int32_t *__restrict__ blk_elem,
-                                                              const uint32_t *__restrict__ inc_sorted,
-                                                              StageArgs G) {
+                                                              const uint32_t *__restrict__ inc_sorted) {
     using L = SharedLayout<BI, MAXE>;
-    static_assert(!STAGED || L::sv >= 32 * kStageMaxNodes + 8 * kStageMaxEdges, "staging area");
     extern __shared__ __align__(16) unsigned char rs_smem[];
     ElemRec *rec = reinterpret_cast<ElemRec *>(rs_smem);
     double *sv = reinterpret_cast<double *>(rs_smem + L::rec);
@@ -523,35 +382,13 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_shared(RBArgs A, const in
         s_rp[r] = A.rp.row_ptr[a0 + r];
         s_ip[r] = A.rp.inc_ptr[a0 + r];
     }
-    // staging (sv is free until phase A2): the block's distinct nodes and edge values,
-    // each gathered once, and this thread's element record
-    double4 *scoord = reinterpret_cast<double4 *>(sv);
-    double *ssol = sv + 4 * kStageMaxNodes;
-    uint4 er = make_uint4(0u, 0u, 0u, 0u);
-    if (STAGED) {
-        const int nn = G.cnt[2 * blockIdx.x], nd = G.cnt[2 * blockIdx.x + 1];
-        const int noff = G.off[3 * blockIdx.x], doff = G.off[3 * blockIdx.x + 1], eoff = G.off[3 * blockIdx.x + 2];
-        if (tid < nel && tid < MAXE) er = __ldg(G.erec + eoff + tid);
-        for (int i = tid; i < nn; i += BI) scoord[i] = A.m.xyz[__ldg(G.node + noff + i)];
-        for (int i = tid; i < nd; i += BI) ssol[i] = __ldg(A.sol + __ldg(G.edge + doff + i));
-        __syncthreads();
-    }
     // phase A1: one thread per distinct element (the plan keeps nel <= MAXE)
     if (tid < nel && tid < MAXE) {
         unsigned sb;
         int tag;
         Geo g;
         double a[6];
-        if (STAGED) {
-            sb = er.w >> 8;
-            tag = (int)(er.w & 0xFF);
-            geometry_v(scoord[er.x & 0xFF], scoord[(er.x >> 8) & 0xFF], scoord[(er.x >> 16) & 0xFF], scoord[er.x >> 24],
-                       g);
-            const unsigned li[6] = {er.y & 0x3FF, (er.y >> 10) & 0x3FF, (er.y >> 20) & 0x3FF,
-                                    er.z & 0x3FF, (er.z >> 10) & 0x3FF, (er.z >> 20) & 0x3FF};
-#pragma unroll
-            for (int i = 0; i < 6; i++) a[i] = li[i] != 0x3FFu ? flip(ssol[li[i]], (sb >> i) & 1) : 0.0;
-        } else {
+        {
             const int64_t e = blk_elem[k0 + tid];
             int4 tt = A.m.tet[e];
             int d[6];
@@ -894,62 +731,6 @@ __global__ void __launch_bounds__(BI, MINB) k_rowblock_nz(RBArgs A, const int32_
 
 }  // namespace
 
-namespace {
-
-void free_stage(RowBlockPlan *p) {
-    void *q[] = {p->stg_cnt, p->stg_off, p->stg_node, p->stg_edge, p->stg_erec};
-    for (void *x : q)
-        if (x) cudaFree(x);
-    p->stg_cnt = p->stg_off = p->stg_node = p->stg_edge = nullptr;
-    p->stg_erec = nullptr;
-    p->staged_ok = 0;
-}
-
-// Staging tables for the shared-element kernel; on any failure the kernel runs unstaged.
-void build_stage(const ElemData &m, RowBlockPlan *out, cudaStream_t s) {
-    const int nb = out->nblocks;
-    std::vector<int32_t> cnt((size_t)2 * nb), nel((size_t)nb);
-    bool ok = cudaMalloc(&out->stg_cnt, (size_t)2 * nb * 4) == cudaSuccess &&
-              cudaMalloc(&out->stg_off, (size_t)3 * nb * 4) == cudaSuccess;
-    if (ok) {
-        k_block_stage<<<nb, kBlockInc, 0, s>>>(m, out->blk_nelem, out->blk_k0, out->blk_elem, 0, out->stg_cnt,
-                                              nullptr, nullptr, nullptr, nullptr);
-        ok = cudaMemcpyAsync(cnt.data(), out->stg_cnt, cnt.size() * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
-             cudaMemcpyAsync(nel.data(), out->blk_nelem, nel.size() * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
-             cudaStreamSynchronize(s) == cudaSuccess;
-    }
-    std::vector<int32_t> off((size_t)3 * nb);
-    int64_t tn = 0, td = 0, te = 0;
-    for (int b = 0; ok && b < nb; b++) {
-        if (cnt[2 * b] > kStageMaxNodes || cnt[2 * b + 1] > kStageMaxEdges) ok = false;
-        off[3 * b] = (int32_t)tn;
-        off[3 * b + 1] = (int32_t)td;
-        off[3 * b + 2] = (int32_t)te;
-        tn += cnt[2 * b];
-        td += cnt[2 * b + 1];
-        te += nel[b];
-    }
-    ok = ok && te < (int64_t)1 << 31 && td < (int64_t)1 << 31;
-    ok = ok && cudaMalloc(&out->stg_node, (size_t)(tn > 0 ? tn : 1) * 4) == cudaSuccess &&
-         cudaMalloc(&out->stg_edge, (size_t)(td > 0 ? td : 1) * 4) == cudaSuccess &&
-         cudaMalloc(&out->stg_erec, (size_t)(te > 0 ? te : 1) * 16) == cudaSuccess &&
-         cudaMemcpyAsync(out->stg_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, s) == cudaSuccess;
-    if (ok) {
-        k_block_stage<<<nb, kBlockInc, 0, s>>>(m, out->blk_nelem, out->blk_k0, out->blk_elem, 1, out->stg_cnt,
-                                              out->stg_off, out->stg_node, out->stg_edge, out->stg_erec);
-        ok = cudaStreamSynchronize(s) == cudaSuccess && cudaGetLastError() == cudaSuccess;
-    }
-    if (!ok) {
-        cudaGetLastError();
-        free_stage(out);
-        return;
-    }
-    out->staged_ok = 1;
-    out->bytes += (int64_t)nb * 20 + (tn + td) * 4 + te * 16;
-}
-
-}  // namespace
-
 int build_second_masks(const RowPlan &rp, int64_t ninc, uint8_t **out, cudaStream_t s) {
     *out = nullptr;
     uint8_t *second = nullptr;
@@ -975,7 +756,7 @@ int build_second_masks(const RowPlan &rp, int64_t ninc, uint8_t **out, cudaStrea
 }
 
 int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc, bool with_shared,
-                        const ElemData *stage_mesh, const uint8_t *second) {
+                        const uint8_t *second) {
     *out = RowBlockPlan{};
     std::vector<int32_t> ip((size_t)rp.ndof + 1), rpp((size_t)rp.ndof + 1);
     MAG_CUDA_TRY(cudaMemcpyAsync(ip.data(), rp.inc_ptr, ip.size() * 4, cudaMemcpyDeviceToHost, s));
@@ -1040,31 +821,12 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
             with_shared = false;
             break;
         }
-        // staging capacity (distinct nodes / edge dofs per block), when the blocks will be staged
-        std::vector<int32_t> scnt;
-        bool elem_over = false;
-        for (int32_t b = 0; b < out->nblocks; b++) elem_over = elem_over || nel[b] > max_elems;
-        if (stage_mesh && !elem_over) {
-            int32_t *d_cnt = nullptr;
-            if (cudaMalloc(&d_cnt, (size_t)2 * out->nblocks * 4) == cudaSuccess) {
-                k_block_stage<<<out->nblocks, kBlockInc, 0, s>>>(*stage_mesh, out->blk_nelem, out->blk_k0,
-                                                                out->blk_elem, 0, d_cnt, nullptr, nullptr, nullptr,
-                                                                nullptr);
-                scnt.resize((size_t)2 * out->nblocks);
-                if (cudaMemcpyAsync(scnt.data(), d_cnt, scnt.size() * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-                    cudaStreamSynchronize(s) != cudaSuccess)
-                    scnt.clear();
-                cudaFree(d_cnt);
-            }
-        }
         std::vector<int32_t> next;
         next.reserve(starts.size() + 16);
         bool split = false;
         for (int32_t b = 0; b < out->nblocks; b++) {
             next.push_back(starts[b]);
-            const bool over = nel[b] > max_elems ||
-                              (!scnt.empty() && (scnt[2 * b] > kStageMaxNodes || scnt[2 * b + 1] > kStageMaxEdges)) ||
-                              (nz && rpp[starts[b + 1]] - rpp[starts[b]] > kNzMaxSpan);
+            const bool over = nel[b] > max_elems || (nz && rpp[starts[b + 1]] - rpp[starts[b]] > kNzMaxSpan);
             if (over && starts[b + 1] - starts[b] > 1) {
                 next.push_back(starts[b] + (starts[b + 1] - starts[b]) / 2);
                 split = true;
@@ -1090,7 +852,6 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
     MAG_CUDA_TRY(cudaStreamSynchronize(s));
     out->ok = 1;
     out->bytes = (int64_t)starts.size() * 4;
-    if (out->shared_ok && stage_mesh) build_stage(*stage_mesh, out, s);
     if (out->shared_ok) {
         out->bytes += (int64_t)out->nblocks * 8 + ninc * 10;
     } else {
@@ -1110,7 +871,6 @@ int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, in
 }
 
 void free_rowblock_plan(RowBlockPlan *p) {
-    free_stage(p);
     if (p->block_row) cudaFree(p->block_row);
     if (p->blk_nelem) cudaFree(p->blk_nelem);
     if (p->blk_k0) cudaFree(p->blk_k0);
@@ -1157,19 +917,16 @@ namespace mag {
 
 int launch_rowblock_shared_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp,
                                     const double *sol, const QuadParams &qp, const MaterialParams &mp, int calcj,
-                                    double *vals, double *res, cudaStream_t s, bool staged_req) {
-    if (!bp.ok || !bp.shared_ok || !qp.standard_curl || (staged_req && !bp.staged_ok)) return MAG_E_UNSUPPORTED;
+                                    double *vals, double *res, cudaStream_t s) {
+    if (!bp.ok || !bp.shared_ok || !qp.standard_curl) return MAG_E_UNSUPPORTED;
     RBArgs A{m, rp, sol, qp, mp, bp.block_row, vals, res};
     const bool wide = rp.wide != 0, q4 = qp.nq == 4 && qp.uniform_w;
-    const StageArgs G{bp.stg_cnt, bp.stg_off, bp.stg_node, bp.stg_edge, bp.stg_erec};
-    const bool staged = staged_req;
 #define MAG_RS(BI_, ME_, MB_, CJ, Q, W)                                                                   \
     do {                                                                                                 \
-        auto kern = staged ? k_rowblock_shared<BI_, ME_, MB_, CJ, Q, W, true>                            \
-                           : k_rowblock_shared<BI_, ME_, MB_, CJ, Q, W, false>;                          \
+        auto kern = k_rowblock_shared<BI_, ME_, MB_, CJ, Q, W>;                                          \
         const int sm = SharedLayout<BI_, ME_>::bytes;                                                    \
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                     \
-        kern<<<bp.nblocks, BI_, sm, s>>>(A, bp.blk_nelem, bp.blk_k0, bp.blk_elem, bp.inc_sorted, G);     \
+        kern<<<bp.nblocks, BI_, sm, s>>>(A, bp.blk_nelem, bp.blk_k0, bp.blk_elem, bp.inc_sorted);        \
     } while (0)
 #define MAG_RS_ALL(BI_, ME_, MB_)                                                                         \
     do {                                                                                                 \

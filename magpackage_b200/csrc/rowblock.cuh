@@ -34,18 +34,8 @@ struct RowBlockPlan {
     // nonzero-pass kernel: every off-diagonal CSR entry has at most two contributions and
     // inc_sorted carries, per incidence and local column, whether it is the second of them
     int nz_ok = 0;
-    // staging: per block its distinct nodes and edge dofs, and per distinct element a
-    // record of local node / edge indices, tag and sign bits (exact offsets per block)
-    int32_t *stg_cnt = nullptr;    // [nblocks][2] nodes, edges
-    int32_t *stg_off = nullptr;    // [nblocks][3] node, edge, element-record offsets
-    int32_t *stg_node = nullptr;   // node ids
-    int32_t *stg_edge = nullptr;   // edge dofs
-    uint4 *stg_erec = nullptr;     // element records
-    int staged_ok = 0;
 };
 
-constexpr int kStageMaxNodes = 192;  // distinct nodes per block the staged kernel holds
-constexpr int kStageMaxEdges = 512;  // distinct edge dofs per block
 
 // Per incidence (row order) bit j: the incidence is the second of the (at most two)
 // contributions to its column j's off-diagonal entry. *out = NULL when some row breaks
@@ -54,8 +44,7 @@ constexpr int kStageMaxEdges = 512;  // distinct edge dofs per block
 int build_second_masks(const RowPlan &rp, int64_t ninc, uint8_t **out, cudaStream_t s);
 // `second`: the masks above, or NULL (no nonzero-pass plan).
 int build_rowblock_plan(const RowPlan &rp, RowBlockPlan *out, cudaStream_t s, int block_inc = kBlockInc,
-                        bool with_shared = false, const ElemData *stage_mesh = nullptr,
-                        const uint8_t *second = nullptr);
+                        bool with_shared = false, const uint8_t *second = nullptr);
 void free_rowblock_plan(RowBlockPlan *p);
 int launch_rowblock_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp, const double *sol,
                              const QuadParams &qp, const MaterialParams &mp, int calcj, double *vals,
@@ -64,7 +53,7 @@ int launch_rowblock_jacobian(const RowBlockPlan &bp, const ElemData &m, const Ro
 // (standard curl table only; needs bp.shared_ok).
 int launch_rowblock_shared_jacobian(const RowBlockPlan &bp, const ElemData &m, const RowPlan &rp,
                                     const double *sol, const QuadParams &qp, const MaterialParams &mp, int calcj,
-                                    double *vals, double *res, cudaStream_t s, bool staged = false);
+                                    double *vals, double *res, cudaStream_t s);
 // Same result, bit for bit: shared-element blocks whose off-diagonal entries are placed
 // by the incidences themselves and stored by one pass over the block's nonzeros; only
 // the diagonal and the residual are summed per row (needs bp.nz_ok).

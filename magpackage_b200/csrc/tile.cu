@@ -1,0 +1,746 @@
+// Tile-block Newton-Jacobian assembly (FP64, sm_100a): one launch, no scratch in HBM,
+// each element evaluated by one thread, about 1.5 times per assembly.
+//
+// Rows (edges) are grouped by the spatial tile of their lower node: nodes are binned
+// into coordinate layers along x, y and z, and 4 x 4 x 4 layers make a tile (a CTA
+// block holds at most kTileMaxNnz nonzeros and kTileMaxInc incidences; larger tiles
+// are cut). A CTA takes one block: its CSR rows, and every element incident to them.
+//   colour phases -- one thread per element evaluates geometry, the six curls, B and
+//              nu(|B|^2) once (the reference's arithmetic), then, for each of its local
+//              rows that belongs to the block, the row of the 6x6 tangent and the
+//              residual entry. Off-diagonal entries go straight into the block's
+//              shared-memory copy of its CSR values as slot = slot + v. An
+//              off-diagonal entry has at most two contributions (the two tetrahedra
+//              that share a face) and (0 + a) + b equals (0 + b) + a bit for bit, so
+//              the order does not matter, only that the two updates never overlap:
+//              the plan colours the block's elements so that no two elements of a
+//              colour share an entry (the face-adjacency graph of a Kuhn mesh is
+//              bipartite: two colours), and the colours run one after another.
+//              Diagonal entries and residual entries go to per-incidence slots.
+//   row phase -- one thread per row sums its diagonal and residual contributions in
+//              ascending element order (the reference's sparse() order).
+//   store phase -- the block's rows form runs of consecutive rows, contiguous in the
+//              CSR; warps store them in chunks, coalesced.
+// No floating-point atomics; results equal the reference's MEX + sparse() bit for bit.
+#include <omp.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "element.cuh"
+#include "tile.cuh"
+
+namespace mag {
+
+namespace {
+
+using namespace elem;
+
+struct TileArgs {
+    const TileBlock *blocks;
+    const uint2 *rows;
+    const uint2 *chunks;
+    const uint4 *recs;
+    int64_t nrec;
+    const double4 *xyz;
+    const double *sol;
+    const double *nu_e;
+    QuadParams qp;
+    MaterialParams mp;
+    double *vals;
+    double *res;
+    int *err;
+    int64_t nnz_total, ndof;
+    int smem_nnz;  // doubles reserved for the block's values (even)
+};
+
+// Sum over the quadrature points of v * w_q (w_q = qw_q |det J|) from zero, in point
+// order. Q4: four equal weights, u = v w_0; the reference's ((u + u) + u) + u equals
+// (3 u) + u because u + u is exact, so 3 u rounds like (u + u) + u.
+template <bool Q4>
+__device__ __forceinline__ double qsum4(double v, const QuadParams &qp, double w0, double adet) {
+    const double u = v * w0;
+    if (Q4) {
+        const double t = 3.0 * u;
+        return t + u;
+    }
+    double acc = u;
+    if (qp.uniform_w) {
+        for (int q = 1; q < qp.nq; q++) acc = acc + u;
+    } else {
+        for (int q = 1; q < qp.nq; q++) acc = acc + v * (qp.qw[q] * adet);
+    }
+    return acc;
+}
+
+__device__ __forceinline__ void flag(int *err) { atomicOr(err, 1); }
+
+// One element of the block: record i. STIFF: K(nu) with the element's given nu.
+template <bool CALCJ, bool Q4, bool STIFF>
+__device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, double *__restrict__ slot,
+                                             double2 *__restrict__ incv, int bnnz, int binc) {
+    const int64_t n = A.nrec;
+    const uint4 p0 = __ldg(A.recs + i), p1 = __ldg(A.recs + n + i), p2 = __ldg(A.recs + 2 * n + i);
+    const uint4 p3 = __ldg(A.recs + 3 * n + i), p4 = __ldg(A.recs + 4 * n + i), p5 = __ldg(A.recs + 5 * n + i);
+    const int4 tt = make_int4((int)p0.x, (int)p0.y, (int)p0.z, (int)p0.w);
+    const unsigned sb = (p2.w >> 8) & 0x3Fu;
+    const unsigned pos[6] = {p3.x, p3.y, p3.z, p3.w, p4.x, p4.y};
+    const unsigned sl[6] = {p4.z, p4.w, p5.x, p5.y, p5.z, p5.w};
+    Geo g;
+    geometry(A.xyz, tt, g);
+    double C[6][3];
+    curls_standard(g, C);
+    double nu, g2 = 0.0, b[6];
+    if (STIFF) {
+        nu = __ldg(A.nu_e + p2.z);
+#pragma unroll
+        for (int j = 0; j < 6; j++) b[j] = 0.0;
+    } else {
+        const int d[6] = {(int)p1.x, (int)p1.y, (int)p1.z, (int)p1.w, (int)p2.x, (int)p2.y};
+        double a[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) a[k] = d[k] >= 0 ? flip(__ldg(A.sol + d[k]), (sb >> k) & 1) : 0.0;
+        double B[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double v = a[0] * C[0][c];
+#pragma unroll
+            for (int k = 1; k < 6; k++) v = v + a[k] * C[k][c];
+            B[c] = v;
+        }
+        double dnu;
+        material_eval(A.mp, (int)(p2.w & 0xFFu), dot3(B, B), nu, dnu);
+#pragma unroll
+        for (int j = 0; j < 6; j++) b[j] = dot3(B, C[j]);
+        g2 = 2.0 * dnu;
+    }
+    const double adet = g.adet, w0 = A.qp.qw[0] * adet;
+#pragma unroll
+    for (int l = 0; l < 6; l++) {
+        const unsigned s = sl[l];
+        if (s == kTileAbsent) continue;
+        const int nzb = (int)(s & 0xFFFFu), is = (int)(s >> 16);
+        const unsigned si = (sb >> l) & 1u;
+        const double rv = STIFF ? 0.0 : flip(qsum4<Q4>(nu * b[l], A.qp, w0, adet), si);
+        double dv = 0.0;
+        if (CALCJ) {
+            double v[6];
+            if (g2 == 0.0) {
+#pragma unroll
+                for (int j = 0; j < 6; j++) v[j] = qsum4<Q4>(nu * dot3(C[l], C[j]), A.qp, w0, adet);
+            } else {
+                const double gl = g2 * b[l];
+#pragma unroll
+                for (int j = 0; j < 6; j++) v[j] = qsum4<Q4>(nu * dot3(C[l], C[j]) + gl * b[j], A.qp, w0, adet);
+            }
+            dv = v[l];  // the diagonal: si ^ si = 0, no flip
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                if (j == l) continue;
+                const unsigned p = (pos[l] >> (5 * j)) & 31u;
+                if (p == (unsigned)kCompactMaxRow) continue;
+                const int k = nzb + (int)p;
+                if (k < bnnz) {
+                    slot[k] = slot[k] + flip(v[j], si ^ ((sb >> j) & 1u));
+                } else {
+                    flag(A.err);
+                }
+            }
+        }
+        if (is < binc) {
+            incv[is] = make_double2(rv, dv);
+        } else {
+            flag(A.err);
+        }
+    }
+}
+
+template <int BT, int MINB, bool CALCJ, bool Q4, bool STIFF>
+__global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A) {
+    extern __shared__ __align__(16) double tile_smem[];
+    const TileBlock *Bp = A.blocks + blockIdx.x;
+    const int nrows = Bp->nrows, row0 = Bp->row0, rec0 = Bp->rec0, nrec = Bp->nrec;
+    const int nnz = Bp->nnz, ninc = Bp->ninc, ncolors = Bp->ncolors;
+    const int chunk0 = Bp->chunk0, nchunks = Bp->nchunks;
+    double *slot = tile_smem;
+    double2 *incv = reinterpret_cast<double2 *>(tile_smem + A.smem_nnz);
+    const int tid = threadIdx.x;
+    if (CALCJ) {
+        for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
+        __syncthreads();
+        int c0 = 0;
+        for (int c = 0; c < ncolors; c++) {
+            const int c1 = Bp->col_end[c];
+            for (int i = c0 + tid; i < c1; i += BT)
+                tile_element<CALCJ, Q4, STIFF>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
+            c0 = c1;
+            __syncthreads();
+        }
+    } else {
+        for (int i = tid; i < nrec; i += BT)
+            tile_element<CALCJ, Q4, STIFF>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
+        __syncthreads();
+    }
+    // rows: diagonal and residual in ascending element order
+    for (int r = tid; r < nrows; r += BT) {
+        const uint2 rw = __ldg(A.rows + row0 + r);
+        const int nzb = (int)(rw.y & 0x1FFFu), incb = (int)((rw.y >> 13) & 0xFFFu);
+        const int diag = (int)((rw.y >> 25) & 31u);
+        int ince = r + 1 < nrows ? (int)((__ldg(&A.rows[row0 + r + 1].y) >> 13) & 0xFFFu) : ninc;
+        if (ince > ninc) ince = ninc;
+        double racc = 0.0, dacc = 0.0;
+        for (int k = incb; k < ince; k++) {
+            const double2 v = incv[k];
+            racc = racc + v.x;
+            if (CALCJ) dacc = dacc + v.y;
+        }
+        if (!STIFF) {
+            if ((int64_t)rw.x < A.ndof) A.res[rw.x] = racc;
+            else flag(A.err);
+        }
+        if (CALCJ && ince > incb) {
+            if (nzb + diag < nnz) slot[nzb + diag] = dacc;
+            else flag(A.err);
+        }
+    }
+    if (CALCJ) {
+        __syncthreads();
+        const int warp = tid >> 5, lane = tid & 31;
+        for (int c = warp; c < nchunks; c += BT / 32) {
+            const uint2 ch = __ldg(A.chunks + chunk0 + c);
+            const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
+            const int64_t g = (int64_t)ch.y;
+            if (sb0 + len > nnz || g + len > A.nnz_total) {
+                if (lane == 0) flag(A.err);
+                continue;
+            }
+            for (int i = lane; i < len; i += 32) A.vals[g + i] = slot[sb0 + i];
+        }
+    }
+}
+
+constexpr int kTileBT = 256;
+constexpr int kTileMinB = 2;
+
+// ---- host plan builder --------------------------------------------------------------
+
+struct HostRec {
+    uint32_t w[24];  // the six 16-byte planes of one record, plane-major
+};
+
+// Layer index of every node along one axis: sorted coordinates split where
+// consecutive values are more than 0.3 h apart or a layer would span more than h.
+void axis_layers(const std::vector<double4> &xyz, int axis, double h, std::vector<int32_t> &layer) {
+    const int64_t n = (int64_t)xyz.size();
+    std::vector<std::pair<double, int32_t>> v((size_t)n);
+    for (int64_t i = 0; i < n; i++) {
+        const double c = axis == 0 ? xyz[i].x : axis == 1 ? xyz[i].y : xyz[i].z;
+        v[i] = {c, (int32_t)i};
+    }
+    std::sort(v.begin(), v.end());
+    layer.assign((size_t)n, 0);
+    int32_t L = 0;
+    double start = n ? v[0].first : 0.0;
+    for (int64_t i = 1; i < n; i++) {
+        const double x = v[i].first;
+        if (x - v[i - 1].first > 0.3 * h || x - start > h) {
+            L++;
+            start = x;
+        }
+        layer[v[i].second] = L;
+    }
+}
+
+template <typename T>
+int download(std::vector<T> &dst, const T *src, int64_t count, cudaStream_t s) {
+    dst.resize((size_t)count);
+    if (count == 0) return MAG_OK;
+    MAG_CUDA_TRY(cudaMemcpyAsync(dst.data(), src, (size_t)count * sizeof(T), cudaMemcpyDeviceToHost, s));
+    return MAG_OK;
+}
+
+}  // namespace
+
+void free_tile_plan(TilePlan *p) {
+    void *q[] = {p->blocks, p->rows, p->chunks, p->recs};
+    for (void *x : q)
+        if (x) cudaFree(x);
+    *p = TilePlan{};
+}
+
+bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
+    *out = TileHostPlan{};
+    const std::vector<double4> &xyz = hm.xyz;
+    const std::vector<int4> &tet = hm.tet;
+    const std::vector<int32_t> &dofs = hm.dofs, &row_ptr = hm.row_ptr, &inc_ptr = hm.inc_ptr;
+    const std::vector<uint8_t> &tags = hm.tags, &sbits = hm.sbits;
+    const std::vector<uint32_t> &inc_elem = hm.inc_elem, &inc_pos = hm.inc_pos;
+    const int64_t ndof = (int64_t)row_ptr.size() - 1, ne = (int64_t)tet.size();
+    const int64_t ninc_total = (int64_t)inc_elem.size();
+    const bool have_signs = !sbits.empty();
+    if (ne <= 0 || ndof <= 0 || hm.nnz >= (int64_t(1) << 32)) return false;
+
+    // an element with a repeated dof would update a diagonal slot or one slot twice
+    for (int64_t e = 0; e < ne; e++)
+        for (int a = 0; a < 6; a++)
+            for (int b = a + 1; b < 6; b++)
+                if (dofs[6 * e + a] >= 0 && dofs[6 * e + a] == dofs[6 * e + b]) return false;
+
+    // ---- spatial layers and tiles ----
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (const double4 &p : xyz) {
+        const double c[3] = {p.x, p.y, p.z};
+        for (int a = 0; a < 3; a++) {
+            lo[a] = std::min(lo[a], c[a]);
+            hi[a] = std::max(hi[a], c[a]);
+        }
+    }
+    double vol = 1.0, ext_max = 0.0;
+    for (int a = 0; a < 3; a++) {
+        vol *= hi[a] - lo[a];
+        ext_max = std::max(ext_max, hi[a] - lo[a]);
+    }
+    const double nn = (double)xyz.size();
+    double h = vol > 0.0 ? std::cbrt(vol / nn) : ext_max / std::max(1.0, std::cbrt(nn));
+    if (!(h > 0.0)) h = 1.0;
+    std::vector<int32_t> layer[3];
+    for (int a = 0; a < 3; a++) axis_layers(xyz, a, h, layer[a]);
+    constexpr int kTileLayers = 4;
+    int32_t ntile[3] = {1, 1, 1};
+    for (int a = 0; a < 3; a++) {
+        int32_t m = 0;
+        for (int32_t v : layer[a]) m = std::max(m, v);
+        ntile[a] = m / kTileLayers + 1;
+    }
+    const int64_t tiles = (int64_t)ntile[0] * ntile[1] * ntile[2];
+    if (tiles >= (int64_t(1) << 31)) return false;
+    // tile of every row: that of its edge's lower node; a row without incidences
+    // (an unused dof) joins the tile of the row before it
+    std::vector<int32_t> row_tile((size_t)ndof, 0);
+    {
+        int32_t prev = 0;
+        for (int64_t r = 0; r < ndof; r++) {
+            if (inc_ptr[r + 1] > inc_ptr[r]) {
+                const uint32_t ew = inc_elem[inc_ptr[r]];
+                const int64_t e = ew & 0x1FFFFFFFu;
+                const int l = (int)(ew >> 29);
+                const int *t = &tet[e].x;
+                const int32_t na = t[edge_a(l)], nb = t[edge_b(l)];
+                const int32_t node = na < nb ? na : nb;
+                prev = (layer[0][node] / kTileLayers) +
+                       ntile[0] * ((layer[1][node] / kTileLayers) + ntile[1] * (layer[2][node] / kTileLayers));
+            }
+            row_tile[r] = prev;
+        }
+    }
+    // rows grouped by tile (stable: ascending ids within a tile)
+    std::vector<int64_t> tstart((size_t)tiles + 1, 0);
+    for (int64_t r = 0; r < ndof; r++) tstart[row_tile[r] + 1]++;
+    for (int64_t t = 0; t < tiles; t++) tstart[t + 1] += tstart[t];
+    std::vector<int32_t> order((size_t)ndof);
+    {
+        std::vector<int64_t> fill(tstart.begin(), tstart.end() - 1);
+        for (int64_t r = 0; r < ndof; r++) order[fill[row_tile[r]]++] = (int32_t)r;
+    }
+    // blocks: each tile's rows, cut where a block would exceed its capacity
+    std::vector<int64_t> bstart;  // index into order
+    for (int64_t t = 0; t < tiles; t++) {
+        int64_t k = tstart[t];
+        const int64_t k1 = tstart[t + 1];
+        while (k < k1) {
+            bstart.push_back(k);
+            int64_t bn = 0, bi = 0;
+            while (k < k1) {
+                const int32_t r = order[k];
+                const int64_t rn = row_ptr[r + 1] - row_ptr[r], ri = inc_ptr[r + 1] - inc_ptr[r];
+                if (rn > kCompactMaxRow || ri > kCompactMaxRow) return false;
+                if (bn + rn > kTileMaxNnz || bi + ri > kTileMaxInc) break;
+                bn += rn;
+                bi += ri;
+                k++;
+            }
+        }
+    }
+    bstart.push_back(ndof);
+    const int64_t nb = (int64_t)bstart.size() - 1;
+    if (nb >= (int64_t(1) << 31)) return false;
+
+    std::vector<TileBlock> blocks((size_t)nb);
+    std::vector<uint2> rows((size_t)ndof);
+    std::vector<std::vector<HostRec>> brec((size_t)nb);
+    std::vector<std::vector<uint2>> bchunk((size_t)nb);
+    std::atomic<int> fail{0};
+
+#pragma omp parallel
+    {
+        struct Inc {
+            int64_t e;
+            int l;
+            int lr;     // block-local row
+            int32_t k;  // incidence index
+        };
+        std::vector<Inc> incs;
+        std::vector<int32_t> own_a, own_b, color, adj_ptr, adj, queue;
+        std::vector<uint8_t> cnt;
+#pragma omp for schedule(dynamic, 16)
+        for (int64_t b = 0; b < nb; b++) {
+            if (fail) continue;
+            const int64_t k0 = bstart[b], k1 = bstart[b + 1];
+            TileBlock &B = blocks[b];
+            std::memset(&B, 0, sizeof B);
+            B.row0 = (int32_t)k0;
+            B.nrows = (int32_t)(k1 - k0);
+            // row table and incidences
+            int32_t bn = 0, bi = 0;
+            incs.clear();
+            for (int64_t k = k0; k < k1; k++) {
+                const int32_t r = order[k];
+                const int32_t rn = row_ptr[r + 1] - row_ptr[r];
+                const int32_t i0 = inc_ptr[r], i1 = inc_ptr[r + 1];
+                uint32_t diag = 0;
+                for (int32_t t = i0; t < i1; t++) {
+                    const uint32_t ew = inc_elem[t];
+                    const int l = (int)(ew >> 29);
+                    if (t == i0) diag = (inc_pos[t] >> (5 * l)) & 31u;
+                    incs.push_back(Inc{(int64_t)(ew & 0x1FFFFFFFu), l, (int)(k - k0), t});
+                }
+                rows[k] = make_uint2((uint32_t)r, (uint32_t)bn | ((uint32_t)bi << 13) | (diag << 25));
+                bn += rn;
+                bi += i1 - i0;
+            }
+            B.nnz = bn;
+            B.ninc = bi;
+            // store chunks: runs of consecutive rows, cut at kTileChunk nonzeros
+            std::vector<uint2> &ch = bchunk[b];
+            ch.clear();
+            {
+                int32_t off = 0;
+                int64_t k = k0;
+                while (k < k1) {
+                    int64_t k2 = k + 1;
+                    while (k2 < k1 && order[k2] == order[k2 - 1] + 1) k2++;
+                    const int64_t g0 = row_ptr[order[k]], g1 = row_ptr[order[k2 - 1] + 1];
+                    for (int64_t g = g0; g < g1; g += kTileChunk) {
+                        const int32_t len = (int32_t)std::min<int64_t>(kTileChunk, g1 - g);
+                        ch.push_back(make_uint2((uint32_t)(off + (g - g0)) | ((uint32_t)len << 16), (uint32_t)g));
+                    }
+                    off += (int32_t)(g1 - g0);
+                    k = k2;
+                }
+            }
+            B.nchunks = (int32_t)ch.size();
+            // distinct elements (ascending) and their records
+            std::sort(incs.begin(), incs.end(), [](const Inc &x, const Inc &y) {
+                return x.e != y.e ? x.e < y.e : x.l < y.l;
+            });
+            std::vector<HostRec> &rec = brec[b];
+            rec.clear();
+            for (size_t q = 0; q < incs.size(); q++) {
+                const Inc &c = incs[q];
+                if (q == 0 || incs[q - 1].e != c.e) {
+                    HostRec h;
+                    const int64_t e = c.e;
+                    const int4 tt = tet[e];
+                    h.w[0] = (uint32_t)tt.x;
+                    h.w[1] = (uint32_t)tt.y;
+                    h.w[2] = (uint32_t)tt.z;
+                    h.w[3] = (uint32_t)tt.w;
+                    for (int j = 0; j < 4; j++) h.w[4 + j] = (uint32_t)dofs[6 * e + j];
+                    h.w[8] = (uint32_t)dofs[6 * e + 4];
+                    h.w[9] = (uint32_t)dofs[6 * e + 5];
+                    h.w[10] = (uint32_t)e;
+                    unsigned sb = 0;
+                    if (have_signs) {
+                        sb = sbits[e];
+                    } else {
+                        const int n4[4] = {tt.x, tt.y, tt.z, tt.w};
+                        for (int j = 0; j < 6; j++) sb |= (n4[edge_a(j)] < n4[edge_b(j)] ? 0u : 1u) << j;
+                    }
+                    h.w[11] = (uint32_t)tags[e] | (sb << 8);
+                    for (int j = 12; j < 18; j++) h.w[j] = 0;
+                    for (int j = 18; j < 24; j++) h.w[j] = kTileAbsent;
+                    rec.push_back(h);
+                } else if (incs[q - 1].l == c.l) {
+                    fail = 1;  // one element twice in a row's incidences at the same local row
+                }
+                HostRec &h = rec.back();
+                const uint2 rw = rows[k0 + c.lr];
+                const int32_t r = order[k0 + c.lr];
+                const uint32_t nzb = rw.y & 0x1FFFu, incb = (rw.y >> 13) & 0xFFFu;
+                h.w[12 + c.l] = inc_pos[c.k];
+                h.w[18 + c.l] = nzb | ((incb + (uint32_t)(c.k - inc_ptr[r])) << 16);
+            }
+            const int32_t nr = (int32_t)rec.size();
+            // colour classes: conflict = two elements updating the same off-diagonal slot
+            own_a.assign((size_t)bn, -1);
+            own_b.assign((size_t)bn, -1);
+            cnt.assign((size_t)bn, 0);
+            for (int32_t i = 0; i < nr && !fail; i++) {
+                const HostRec &h = rec[i];
+                for (int l = 0; l < 6; l++) {
+                    if (h.w[18 + l] == kTileAbsent) continue;
+                    const uint32_t nzb = h.w[18 + l] & 0xFFFFu;
+                    for (int j = 0; j < 6; j++) {
+                        if (j == l) continue;
+                        const uint32_t p = (h.w[12 + l] >> (5 * j)) & 31u;
+                        if (p == (uint32_t)kCompactMaxRow) continue;
+                        const uint32_t sl = nzb + p;
+                        if (sl >= (uint32_t)bn || cnt[sl] >= 2) {
+                            fail = 1;
+                            break;
+                        }
+                        if (cnt[sl] == 0) own_a[sl] = i;
+                        else own_b[sl] = i;
+                        cnt[sl]++;
+                    }
+                }
+            }
+            if (fail) continue;
+            // adjacency (CSR over records)
+            adj_ptr.assign((size_t)nr + 1, 0);
+            for (int32_t sl = 0; sl < bn; sl++)
+                if (cnt[sl] == 2) {
+                    adj_ptr[own_a[sl] + 1]++;
+                    adj_ptr[own_b[sl] + 1]++;
+                }
+            for (int32_t i = 0; i < nr; i++) adj_ptr[i + 1] += adj_ptr[i];
+            adj.assign((size_t)adj_ptr[nr], 0);
+            {
+                std::vector<int32_t> f(adj_ptr.begin(), adj_ptr.end() - 1);
+                for (int32_t sl = 0; sl < bn; sl++)
+                    if (cnt[sl] == 2) {
+                        adj[f[own_a[sl]]++] = own_b[sl];
+                        adj[f[own_b[sl]]++] = own_a[sl];
+                    }
+            }
+            // two colours by breadth-first search where the graph is bipartite (components
+            // flipped to balance the classes), else greedy in element order
+            color.assign((size_t)nr, -1);
+            bool two = true;
+            int64_t size0 = 0, size1 = 0;
+            for (int32_t s0 = 0; s0 < nr && two; s0++) {
+                if (color[s0] >= 0) continue;
+                queue.clear();
+                queue.push_back(s0);
+                color[s0] = 0;
+                int64_t c0 = 1, c1 = 0;
+                for (size_t qh = 0; qh < queue.size() && two; qh++) {
+                    const int32_t u = queue[qh];
+                    for (int32_t t = adj_ptr[u]; t < adj_ptr[u + 1]; t++) {
+                        const int32_t w = adj[t];
+                        if (color[w] < 0) {
+                            color[w] = 1 - color[u];
+                            (color[w] ? c1 : c0)++;
+                            queue.push_back(w);
+                        } else if (color[w] == color[u]) {
+                            two = false;
+                            break;
+                        }
+                    }
+                }
+                if (two && std::llabs((size0 + c1) - (size1 + c0)) < std::llabs((size0 + c0) - (size1 + c1))) {
+                    for (int32_t u : queue) color[u] = 1 - color[u];
+                    std::swap(c0, c1);
+                }
+                size0 += c0;
+                size1 += c1;
+            }
+            int ncol = 2;
+            if (!two) {
+                color.assign((size_t)nr, -1);
+                ncol = 0;
+                for (int32_t u = 0; u < nr; u++) {
+                    unsigned used = 0;
+                    for (int32_t t = adj_ptr[u]; t < adj_ptr[u + 1]; t++)
+                        if (color[adj[t]] >= 0) used |= 1u << color[adj[t]];
+                    int c = 0;
+                    while (c < 32 && (used >> c) & 1u) c++;
+                    color[u] = c;
+                    ncol = std::max(ncol, c + 1);
+                }
+                if (ncol > kTileMaxColors) {
+                    fail = 1;
+                    continue;
+                }
+            }
+            // records by colour, ascending element within a colour
+            std::vector<int32_t> idx((size_t)nr);
+            for (int32_t i = 0; i < nr; i++) idx[i] = i;
+            std::stable_sort(idx.begin(), idx.end(), [&](int32_t x, int32_t y) { return color[x] < color[y]; });
+            std::vector<HostRec> sorted((size_t)nr);
+            for (int32_t i = 0; i < nr; i++) sorted[i] = rec[idx[i]];
+            rec.swap(sorted);
+            B.nrec = nr;
+            B.ncolors = ncol;
+            for (int c = 0; c < kTileMaxColors; c++) B.col_end[c] = 0;
+            for (int32_t i = 0; i < nr; i++) B.col_end[color[idx[i]]] = i + 1;
+            for (int c = 1; c < ncol; c++) B.col_end[c] = std::max(B.col_end[c], B.col_end[c - 1]);
+        }
+    }
+    if (fail) return false;
+
+    // concatenate: record and chunk offsets, planes
+    int64_t nrec = 0, nch = 0;
+    int32_t max_nnz = 0, max_inc = 0, max_col = 0;
+    for (int64_t b = 0; b < nb; b++) {
+        blocks[b].rec0 = (int32_t)nrec;
+        blocks[b].chunk0 = (int32_t)nch;
+        nrec += blocks[b].nrec;
+        nch += blocks[b].nchunks;
+        max_nnz = std::max(max_nnz, blocks[b].nnz);
+        max_inc = std::max(max_inc, blocks[b].ninc);
+        max_col = std::max(max_col, blocks[b].ncolors);
+        if (nrec >= (int64_t(1) << 31) || nch >= (int64_t(1) << 31)) return false;
+    }
+    std::vector<uint4> planes((size_t)(6 * nrec));
+    std::vector<uint2> chunks((size_t)nch);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t b = 0; b < nb; b++) {
+        const std::vector<HostRec> &rec = brec[b];
+        const int64_t o = blocks[b].rec0;
+        for (size_t i = 0; i < rec.size(); i++)
+            for (int k = 0; k < 6; k++) {
+                const uint32_t *w = rec[i].w + 4 * k;
+                planes[(size_t)k * nrec + o + i] = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        std::copy(bchunk[b].begin(), bchunk[b].end(), chunks.begin() + blocks[b].chunk0);
+    }
+    // coverage check: every incidence is one record slot
+    {
+        int64_t present = 0;
+        for (int64_t i = 0; i < nrec; i++) {
+            const uint4 a = planes[4 * nrec + i], c = planes[5 * nrec + i];
+            const uint32_t sl[6] = {a.z, a.w, c.x, c.y, c.z, c.w};
+            for (int l = 0; l < 6; l++) present += sl[l] != kTileAbsent;
+        }
+        if (present != ninc_total) return false;
+    }
+    out->blocks.swap(blocks);
+    out->rows.swap(rows);
+    out->chunks.swap(chunks);
+    out->planes.swap(planes);
+    out->nrec = nrec;
+    out->max_nnz = max_nnz;
+    out->max_inc = max_inc;
+    out->max_colors = max_col;
+    return true;
+}
+
+int build_tile_plan(const TilePlanInput &in, TilePlan *plan, cudaStream_t s) {
+    *plan = TilePlan{};
+    if (in.wide || in.ne <= 0 || in.ndof <= 0 || in.nnz >= (int64_t(1) << 32)) return MAG_OK;
+    const auto t_start = std::chrono::steady_clock::now();
+    TileHostMesh hm;
+    MAG_TRY(download(hm.xyz, in.xyz, in.nn, s));
+    MAG_TRY(download(hm.tet, in.tet, in.ne, s));
+    MAG_TRY(download(hm.dofs, in.dofs, 6 * in.ne, s));
+    MAG_TRY(download(hm.tags, in.tags, in.ne, s));
+    if (in.signbits) MAG_TRY(download(hm.sbits, in.signbits, in.ne, s));
+    MAG_TRY(download(hm.row_ptr, in.row_ptr, in.ndof + 1, s));
+    MAG_TRY(download(hm.inc_ptr, in.inc_ptr, in.ndof + 1, s));
+    MAG_TRY(download(hm.inc_elem, in.inc_elem, in.ninc, s));
+    MAG_TRY(download(hm.inc_pos, in.inc_pos, in.ninc, s));
+    MAG_CUDA_TRY(cudaStreamSynchronize(s));
+    hm.nnz = in.nnz;
+    TileHostPlan hp;
+    if (!plan_tiles_host(hm, &hp)) return MAG_OK;
+    TilePlan p;
+    const int64_t nb = (int64_t)hp.blocks.size(), nch = (int64_t)hp.chunks.size(), nrec = hp.nrec;
+    p.nblocks = (int32_t)nb;
+    p.nrows = in.ndof;
+    p.nchunks = nch;
+    p.nrec = nrec;
+    p.nnz = in.nnz;
+    p.max_nnz = hp.max_nnz;
+    p.max_inc = hp.max_inc;
+    p.max_colors = hp.max_colors;
+    p.evals_per_elem = (double)nrec / (double)in.ne;
+    const size_t b_blk = (size_t)nb * sizeof(TileBlock), b_rows = hp.rows.size() * sizeof(uint2),
+                 b_ch = (size_t)std::max<int64_t>(nch, 1) * sizeof(uint2),
+                 b_rec = (size_t)std::max<int64_t>(6 * nrec, 1) * sizeof(uint4);
+    if (cudaMalloc(&p.blocks, b_blk) != cudaSuccess || cudaMalloc(&p.rows, b_rows) != cudaSuccess ||
+        cudaMalloc(&p.chunks, b_ch) != cudaSuccess || cudaMalloc(&p.recs, b_rec) != cudaSuccess) {
+        free_tile_plan(&p);
+        cudaGetLastError();
+        return MAG_OK;  // no room: the other schedules remain
+    }
+    MAG_CUDA_TRY(cudaMemcpyAsync(p.blocks, hp.blocks.data(), b_blk, cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(p.rows, hp.rows.data(), b_rows, cudaMemcpyHostToDevice, s));
+    if (nch) MAG_CUDA_TRY(cudaMemcpyAsync(p.chunks, hp.chunks.data(), nch * sizeof(uint2), cudaMemcpyHostToDevice, s));
+    if (nrec)
+        MAG_CUDA_TRY(cudaMemcpyAsync(p.recs, hp.planes.data(), 6 * nrec * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaStreamSynchronize(s));
+    p.bytes = (int64_t)(b_blk + b_rows + b_ch + b_rec);
+    p.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    p.ok = 1;
+    *plan = p;
+    return MAG_OK;
+}
+
+namespace {
+
+size_t tile_smem_bytes(const TilePlan &tp, int *smem_nnz) {
+    *smem_nnz = (tp.max_nnz + 1) & ~1;
+    return (size_t)*smem_nnz * sizeof(double) + (size_t)tp.max_inc * sizeof(double2);
+}
+
+template <bool CALCJ, bool Q4, bool STIFF>
+int launch(const TileArgs &a, const TilePlan &tp, size_t smem, cudaStream_t s) {
+    auto kern = k_tile<kTileBT, kTileMinB, CALCJ, Q4, STIFF>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return MAG_E_CUDA;
+    kern<<<tp.nblocks, kTileBT, smem, s>>>(a);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+TileArgs make_args(const TilePlan &tp, const ElemData &m, const QuadParams &qp, int *err) {
+    TileArgs a{};
+    a.blocks = tp.blocks;
+    a.rows = tp.rows;
+    a.chunks = tp.chunks;
+    a.recs = tp.recs;
+    a.nrec = tp.nrec;
+    a.xyz = m.xyz;
+    a.qp = qp;
+    a.err = err;
+    a.ndof = tp.nrows;
+    return a;
+}
+
+}  // namespace
+
+int launch_tile_jacobian(const TilePlan &tp, const ElemData &m, const double *sol, const QuadParams &qp,
+                         const MaterialParams &mp, int calc_j, double *vals, double *res, int *err,
+                         cudaStream_t s) {
+    if (!tp.ok || !qp.standard_curl) return MAG_E_UNSUPPORTED;
+    TileArgs a = make_args(tp, m, qp, err);
+    a.sol = sol;
+    a.mp = mp;
+    a.vals = vals;
+    a.res = res;
+    a.nnz_total = tp.nnz;
+    size_t smem = tile_smem_bytes(tp, &a.smem_nnz);
+    const bool q4 = qp.nq == 4 && qp.uniform_w;
+    if (calc_j) return q4 ? launch<true, true, false>(a, tp, smem, s) : launch<true, false, false>(a, tp, smem, s);
+    return q4 ? launch<false, true, false>(a, tp, smem, s) : launch<false, false, false>(a, tp, smem, s);
+}
+
+int launch_tile_stiffness(const TilePlan &tp, const ElemData &m, const double *nu, const QuadParams &qp,
+                          double *vals, int *err, cudaStream_t s) {
+    if (!tp.ok || !qp.standard_curl) return MAG_E_UNSUPPORTED;
+    TileArgs a = make_args(tp, m, qp, err);
+    a.nu_e = nu;
+    a.vals = vals;
+    a.nnz_total = tp.nnz;
+    size_t smem = tile_smem_bytes(tp, &a.smem_nnz);
+    const bool q4 = qp.nq == 4 && qp.uniform_w;
+    return q4 ? launch<true, true, true>(a, tp, smem, s) : launch<true, false, true>(a, tp, smem, s);
+}
+
+}  // namespace mag

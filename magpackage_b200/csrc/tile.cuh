@@ -1,0 +1,108 @@
+// Tile-block assembly schedule: plan and launcher (see tile.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mag {
+
+constexpr int kTileMaxNnz = 8191;   // CSR nonzeros per block (13-bit offsets in the row table)
+constexpr int kTileMaxInc = 4095;   // (row, element) incidences per block (12-bit offsets)
+constexpr int kTileMaxColors = 8;   // element colour classes per block
+constexpr int kTileChunk = 256;     // nonzeros per store chunk (one warp stores a chunk)
+constexpr uint32_t kTileAbsent = 0xFFFFFFFFu;
+
+// One CTA's work: whole CSR rows whose edges start in one spatial tile of nodes, and
+// every element incident to those rows, in colour classes.
+struct TileBlock {
+    int32_t row0, nrows;        // entries of TilePlan::rows
+    int32_t rec0, nrec;         // records (elements of the block, sorted by colour then id)
+    int32_t chunk0, nchunks;    // store chunks
+    int32_t nnz, ninc;          // shared-memory extents
+    int32_t ncolors;
+    int32_t col_end[kTileMaxColors];  // record count at the end of each colour class
+    int32_t pad[3];
+};
+static_assert(sizeof(TileBlock) == 80, "TileBlock layout");
+
+// Device plan. Records are 96 bytes in six 16-byte planes (plane k of record i at
+// recs[k * nrec_total + i]) so that a warp's loads of one plane are contiguous:
+//   plane 0: tet (4 node ids)
+//   plane 1: dofs 0..3
+//   plane 2: dofs 4, 5, element id, tag | sign bits << 8
+//   plane 3: per local row 0..3 its six 5-bit in-row column positions (31 = no dof)
+//   plane 4: positions of local rows 4, 5; slots of local rows 0, 1
+//   plane 5: slots of local rows 2..5
+// where a slot is (row's first nonzero in the block) | (incidence slot << 16), or
+// kTileAbsent when the row is not one of the block's.
+// rows: per block row (ascending ids) x = global row, y = nonzero base (13 bits) |
+// incidence base (12 bits) << 13 | diagonal position (5 bits) << 25.
+// chunks: x = block nonzero base | length << 16, y = global nonzero base.
+struct TilePlan {
+    TileBlock *blocks = nullptr;
+    uint2 *rows = nullptr;
+    uint2 *chunks = nullptr;
+    uint4 *recs = nullptr;
+    int32_t nblocks = 0;
+    int64_t nrows = 0, nchunks = 0, nrec = 0, nnz = 0;
+    int32_t max_nnz = 0, max_inc = 0, max_colors = 0;
+    double evals_per_elem = 0.0;  // records / elements
+    double build_ms = 0.0;
+    int64_t bytes = 0;
+    int ok = 0;
+};
+
+struct TilePlanInput {
+    const double4 *xyz;      // device [Nn]
+    const int4 *tet;         // device [Ne]
+    const int32_t *dofs;     // device [Ne][6]
+    const uint8_t *tags;     // device [Ne]
+    const uint8_t *signbits; // device [Ne] or NULL (derived from tet)
+    const int32_t *row_ptr, *inc_ptr;
+    const uint32_t *inc_elem, *inc_pos;
+    int64_t nn, ne, ndof, nnz, ninc;
+    int wide;
+};
+
+// Host copies of what the planner reads (the device mesh and incidence plan).
+struct TileHostMesh {
+    std::vector<double4> xyz;
+    std::vector<int4> tet;
+    std::vector<int32_t> dofs, row_ptr, inc_ptr;
+    std::vector<uint8_t> tags, sbits;  // sbits empty: signs derived from tet
+    std::vector<uint32_t> inc_elem, inc_pos;
+    int64_t nnz = 0;
+};
+
+// The plan's arrays on the host, in the device layout.
+struct TileHostPlan {
+    std::vector<TileBlock> blocks;
+    std::vector<uint2> rows, chunks;
+    std::vector<uint4> planes;  // 6 * nrec
+    int64_t nrec = 0;
+    int32_t max_nnz = 0, max_inc = 0, max_colors = 0;
+};
+
+// The planner itself (host only): false when the mesh does not suit the schedule.
+bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out);
+
+// Builds the plan on the host from the mesh's incidence plan (copied down once).
+// Leaves plan->ok = 0 (and returns MAG_OK) when the mesh does not suit the schedule:
+// wide rows (> 31 entries), an off-diagonal entry with more than two contributions
+// (repeated dofs), or a block needing more than kTileMaxColors colours.
+int build_tile_plan(const TilePlanInput &in, TilePlan *plan, cudaStream_t s);
+void free_tile_plan(TilePlan *plan);
+
+// Jacobian (calc_j) and residual; vals may be NULL when !calc_j.
+int launch_tile_jacobian(const TilePlan &tp, const ElemData &m, const double *sol, const QuadParams &qp,
+                         const MaterialParams &mp, int calc_j, double *vals, double *res, int *err,
+                         cudaStream_t s);
+// K(nu) with per-element reluctivity nu [Ne].
+int launch_tile_stiffness(const TilePlan &tp, const ElemData &m, const double *nu, const QuadParams &qp,
+                          double *vals, int *err, cudaStream_t s);
+
+}  // namespace mag

@@ -72,7 +72,7 @@ class AssemblyPlan:
         self._materials_key = key
 
     def set_schedule(self, schedule: int):
-        """Jacobian schedule: _lib.SCHEDULE_TWO_PASS, SCHEDULE_L2_RING or SCHEDULE_ROW_BLOCKS."""
+        """Jacobian schedule: one of _lib.SCHEDULE_* (all give the same bits)."""
         _lib.check(self._lib.mag_mesh_set_option(self._h, 1, int(schedule)))
         info = _lib.MeshInfo()
         _lib.check(self._lib.mag_mesh_get_info(self._h, C.byref(info)))

@@ -151,3 +151,51 @@ def test_source_and_winding_gateways(gateways, oracle_port):
         out = gateways["winding"](2, m.P, m.T, m.Dofs, m.Signs, m.Tags, float(synth.IRON), f,
                                   np.array([0.0, 0.0, 1.0]), 5e4, qw, val)
         assert bits_equal(out[0]["pr"], I) and bits_equal(out[1]["pr"], V)
+
+
+def test_gateway_mesh_cache_reuse_and_invalidation(gateways, oracle_port):
+    """The MEX entry points keep the converted mesh between calls. A repeated call (the
+    Newton loop's case) returns the same bits from the cached mesh; a coordinate changed in
+    place, a tag changed in place and a dof array changed in place (same addresses, same
+    sizes) are each converted afresh, so every result equals the oracle's for the arrays as
+    they are at that call."""
+    import ctypes as C
+
+    from magpackage_b200 import _lib
+
+    L = _lib.lib()
+    _lib.check(L.mag_mex_cache_clear())
+    m, E, sol, _ = _case(oracle_port, 5, 21)
+    qw, val, curl = quadrature.reference_data(2)
+    pk = material.pack_material_data(synth.standard_materials())
+    gw = gateways["jacobian"]
+
+    def check_against_oracle():
+        I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, qw, curl, pk, True)
+        Jm, Rm = gw(2, *_jac_args(m, sol, pk, qw, curl, True), 1.0)
+        _assert_sparse(Jm, _matlab_sparse(oracle_port, I, J, V, E), E)
+        out = gw(5, *_jac_args(m, sol, pk, qw, curl, True))
+        for o, ref in zip(out, (I, J, V, Ri, Rv)):
+            assert bits_equal(o["pr"], ref)
+        return Jm["pr"].copy()
+
+    first = check_against_oracle()
+    assert bits_equal(check_against_oracle(), first)  # from the cache
+    # a node moved in place (interior node, small move keeps every element valid)
+    node = int(m.T[len(m.T) // 2, 0]) - 1
+    m.P[node] += np.array([1e-3, -2e-3, 1.5e-3]) / 5
+    moved = check_against_oracle()
+    assert not bits_equal(moved, first)
+    # a region tag changed in place: iron <-> air somewhere
+    k = int(np.flatnonzero(m.Tags == synth.IRON)[0])
+    m.Tags[k] = float(synth.AIR)
+    check_against_oracle()
+    # a dof removed in place (0 = no unknown on that edge)
+    m.Dofs[3, 2] = 0.0
+    check_against_oracle()
+    # the curl-curl gateway shares the cached mesh (no tags needed) and stays exact
+    nu = np.random.default_rng(2).uniform(0.5, 2.0, m.ne) * material.NU0
+    I, J, Vk = oracle_port.curl_curl(m, nu, qw, curl)
+    out = gateways["curl_curl"](3, m.P, m.T, m.Dofs, m.Signs, nu, qw, curl)
+    assert bits_equal(out[2]["pr"], Vk)
+    _lib.check(L.mag_mex_cache_clear())

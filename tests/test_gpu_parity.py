@@ -351,22 +351,34 @@ def test_errors_are_reported(oracle_port):
 
 # ---- the three Jacobian schedules ------------------------------------------------------------
 
-SCHEDULES = (_lib.SCHEDULE_SHARED_ROW_BLOCKS, _lib.SCHEDULE_NZ_ROW_BLOCKS, _lib.SCHEDULE_STAGED_ROW_BLOCKS,
-             _lib.SCHEDULE_ROW_BLOCKS, _lib.SCHEDULE_L2_RING, _lib.SCHEDULE_TWO_PASS)
+SCHEDULES = (_lib.SCHEDULE_TILE_BLOCKS, _lib.SCHEDULE_SHARED_ROW_BLOCKS, _lib.SCHEDULE_NZ_ROW_BLOCKS,
+             _lib.SCHEDULE_ROW_BLOCKS, _lib.SCHEDULE_TWO_PASS)
+
+
+def available(plan):
+    """The schedules this mesh supports (the tile and nonzero-pass ones need rows of at most
+    31 entries and off-diagonal entries of at most two contributions)."""
+    out = []
+    for sch in SCHEDULES:
+        if sch == _lib.SCHEDULE_TILE_BLOCKS and plan.info.tile_blocks == 0:
+            continue
+        if sch == _lib.SCHEDULE_NZ_ROW_BLOCKS and plan.info.nz_pass == 0:
+            continue
+        out.append(sch)
+    return out
 
 
 @pytest.mark.parametrize("n,seed", [(13, 21), (30, 22)])
 def test_schedules_agree_bit_for_bit(oracle_port, n, seed):
-    """Shared-element row blocks (default), per-incidence row blocks, the persistent L2-ring
-    launch (ring reused many times at 30^3) and the two-pass kernels give the same bits as
-    each other and as the oracle, with and without the Jacobian, on the fast and the general
-    quadrature path."""
+    """Tile blocks (default), the row-block variants and the two-pass kernels give the same
+    bits as each other and as the oracle, with and without the Jacobian, on the fast and the
+    general quadrature path."""
     mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, n, seed)
     plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
-    assert plan.info.schedule == _lib.SCHEDULE_NZ_ROW_BLOCKS and plan.info.shared_staged == 0
-    assert plan.info.nz_pass == 1
-    if n >= 30:
-        assert 2 * plan.info.fused_ring_tiles < (mesh.num_elements + 255) // 256
+    assert plan.info.schedule == _lib.SCHEDULE_TILE_BLOCKS
+    assert plan.info.nz_pass == 1 and plan.info.tile_colors == 2
+    # 4x4x4-node tiles: each element is evaluated about 1.5 times (1 + 2/4 for interior tiles)
+    assert 1.0 < plan.info.tile_evals_per_elem < 1.75
     pk = material.pack_material_data(synth.standard_materials())
     plan.set_materials(pk)
     x = dev(sol)
@@ -381,10 +393,8 @@ def test_schedules_agree_bit_for_bit(oracle_port, n, seed):
     for name, w in (("std", qw), ("general", qw2)):
         plan.set_quadrature(w, curl, val)
         mat, vec, vec0 = refs[name]
-        for sch in SCHEDULES:
+        for sch in available(plan):
             plan.set_schedule(sch)
-            if sch == _lib.SCHEDULE_STAGED_ROW_BLOCKS:
-                assert plan.info.shared_staged == 1  # built on request
             v, r = plan.jacobian(x)
             _, r0 = plan.jacobian(x, calc_j=False)
             plan.check()
@@ -507,7 +517,8 @@ def test_wide_rows_match_oracle_on_every_schedule(oracle_port):
     assert plan.info.wide_positions == 1 and plan.info.max_row_nnz > 31 and plan.info.nz_pass == 1
     plan.set_materials(pk)
     x = dev(sol)
-    for sch in SCHEDULES:
+    assert plan.info.tile_blocks == 0  # wide rows: the tile schedule is not offered
+    for sch in available(plan):
         plan.set_schedule(sch)
         v, r = plan.jacobian(x)
         plan.check()
@@ -577,13 +588,58 @@ def test_stiffness_nonzero_pass_matches_oracle(oracle_port):
         E = edges.shape[0]
         nu = np.random.default_rng(T.shape[0]).uniform(0.2, 5.0, T.shape[0]) * material.NU0
         plan = AssemblyPlan(P, T, t2e, E, tags, sign)
-        assert plan.info.schedule == _lib.SCHEDULE_NZ_ROW_BLOCKS
+        assert plan.info.schedule in (_lib.SCHEDULE_TILE_BLOCKS, _lib.SCHEDULE_NZ_ROW_BLOCKS)
         for w in (qw, qw2):
             plan.set_quadrature(w, curl, val)
             I, J, V = oracle_port.curl_curl(m, nu, w, curl)
             ref = oracle_matrix(oracle_port, I, J, V, E, False)
+            if plan.info.tile_blocks:
+                plan.set_schedule(_lib.SCHEDULE_TILE_BLOCKS)
+                assert_csr_equal(plan.row_ptr, plan.col_idx, plan.stiffness(dev(nu)), ref)
             plan.set_schedule(_lib.SCHEDULE_NZ_ROW_BLOCKS)
             k_nz = plan.stiffness(dev(nu))
             assert_csr_equal(plan.row_ptr, plan.col_idx, k_nz, ref)
             plan.set_schedule(_lib.SCHEDULE_TWO_PASS)
             assert torch.equal(plan.stiffness(dev(nu)), k_nz)
+
+
+def test_tile_schedule_shuffled_numbering_and_unused_dofs(oracle_port):
+    """The tile schedule on a mesh whose node and element numbering is shuffled (a block's
+    rows are then scattered over the CSR in short runs) with three unused dofs at the end
+    (rows without incidences, whose residual is 0): Jacobian, residual-only pass and K(nu)
+    equal the oracle bit for bit, and a repeated call gives the same bits."""
+    base = synth.kuhn_box(9, 8, 7, seed=4)
+    rng = np.random.default_rng(4)
+    perm = rng.permutation(base.num_nodes)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(perm.size)
+    P = base.P[perm]
+    T = inv[base.T][rng.permutation(base.num_elements)].astype(np.int32)
+    mesh = synth.BoxMesh(P=P, T=T, shape=base.shape, size=base.size)
+    tags = synth.cube_layout(mesh)
+    edges, t2e, sign, m = make_case(oracle_port, P, T, tags)
+    E = edges.shape[0]
+    n = E + 3
+    sol = np.random.default_rng(9).normal(0, 0.05, n) * 10.0 ** np.random.default_rng(8).uniform(-1.5, 0.5, n)
+    pk = material.pack_material_data(synth.standard_materials())
+    qw, val, curl = quadrature.reference_data(2)
+    plan = AssemblyPlan(P, T, t2e, n, tags, sign)
+    plan.set_materials(pk)
+    assert plan.info.schedule == _lib.SCHEDULE_TILE_BLOCKS and plan.info.tile_colors == 2
+    x = dev(sol)
+    I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, qw, curl, pk, True)
+    v, r = plan.jacobian(x)
+    _, r0 = plan.jacobian(x, calc_j=False)
+    plan.check()
+    assert_csr_equal(plan.row_ptr, plan.col_idx, v, oracle_matrix(oracle_port, I, J, V, n, False))
+    rr = oracle_port.sparse_vec(Ri, Rv, n)
+    assert bits_equal(host(r), rr) and bits_equal(host(r0), rr)
+    assert np.all(host(r)[E:] == 0.0)
+    v2, r2 = plan.jacobian(x)
+    assert torch.equal(v.view(torch.int64), v2.view(torch.int64)) and torch.equal(r.view(torch.int64),
+                                                                                   r2.view(torch.int64))
+    nu = np.random.default_rng(5).uniform(0.2, 5.0, T.shape[0]) * material.NU0
+    Ik, Jk, Vk = oracle_port.curl_curl(m, nu, qw, curl)
+    assert_csr_equal(plan.row_ptr, plan.col_idx, plan.stiffness(dev(nu)), oracle_matrix(oracle_port, Ik, Jk, Vk, n, False))
+    plan.check()
+    plan.close()
