@@ -634,6 +634,11 @@ int mag_assemble_jacobian_seeded(mag_mesh *m, const double *d_sol, const double 
         return MAG_E_UNSUPPORTED;
     }
     cudaStream_t s = (cudaStream_t)stream;
+    if (m->schedule == MAG_SCHEDULE_TILE_BLOCKS && m->tile.ok) {
+        MAG_TRY(launch_tile_seeded(m->tile, m->elems(), d_sol, d_bscale, m->qp, m->mat.mp, d_vals, d_res, m->status,
+                                   s));
+        return finish(s);
+    }
     MAG_TRY(launch_jacobian_seeded_elems(m->elems(), d_sol, d_bscale, m->qp, m->mat.mp, m->scratch, s));
     MAG_TRY(launch_rows_reduce(m->rows(), m->pat.max_row, m->scratch, d_vals, d_res, s));
     return finish(s);

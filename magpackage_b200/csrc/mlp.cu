@@ -184,6 +184,74 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem, const float *bias
     }
 }
 
+// ---- inference epilogue: packed FP32 pairs (f32x2) ---------------------------------
+
+__device__ __forceinline__ uint64_t pk2(float a, float b) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void upk2(uint64_t v, float &a, float &b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// SiLU of a hidden pair (z0, z1), packed as BF16 (z0 in the low half): z * (1/2 + tanh(z/2)/2)
+// with the pair's tanh in one half-precision MUFU operation. Its error (about 2^-11 of the
+// sigmoid, as the single-precision tanh.approx has) stays below the BF16 rounding that the
+// next layer's input gets; it halves the transcendental operations of the hidden layers.
+__device__ __forceinline__ uint32_t silu2_bf16(uint64_t z) {
+    constexpr uint32_t kHalf2 = 0x38003800u;  // (0.5, 0.5) in f16x2
+    float z0, z1;
+    upk2(z, z0, z1);
+    uint32_t h;
+    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(h) : "f"(z1), "f"(z0));
+    asm("mul.rn.f16x2 %0, %0, %1;" : "+r"(h) : "r"(kHalf2));
+    asm("tanh.approx.f16x2 %0, %0;" : "+r"(h));
+    asm("fma.rn.f16x2 %0, %0, %1, %1;" : "+r"(h) : "r"(kHalf2));
+    float s0, s1;
+    asm("{\n\t.reg .f16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\tcvt.f32.f16 %0, lo;\n\tcvt.f32.f16 %1, hi;\n\t}"
+        : "=f"(s0), "=f"(s1)
+        : "r"(h));
+    float p0, p1;
+    upk2(mul2(z, pk2(s0, s1)), p0, p1);
+    uint32_t out;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(out) : "f"(p1), "f"(p0));
+    return out;
+}
+
+// Inference form of hidden_epilogue: the same image, packed arithmetic.
+__device__ __forceinline__ void hidden_epilogue_infer(uint32_t tmem, const float *bias, __nv_bfloat16 *img,
+                                                      int row_t) {
+#pragma unroll
+    for (int c = 0; c < kH; c += 16) {
+        float z[16];
+        tmem_cols16(tmem, c, z);
+        __align__(16) uint32_t hp[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const float2 b = *reinterpret_cast<const float2 *>(bias + c + 2 * i);
+            hp[i] = silu2_bf16(add2(pk2(z[2 * i], z[2 * i + 1]), pk2(b.x, b.y)));
+        }
+        *reinterpret_cast<uint4 *>(img + core_off(row_t, c, kH)) = *reinterpret_cast<uint4 *>(hp);
+        *reinterpret_cast<uint4 *>(img + core_off(row_t, c + 8, kH)) = *reinterpret_cast<uint4 *>(hp + 4);
+    }
+}
+
 // Write this thread's row of 64 values as BF16 into a K=64 core-matrix image.
 __device__ __forceinline__ void put_row64(__nv_bfloat16 *img, int row, const float v[kH]) {
 #pragma unroll
@@ -253,6 +321,8 @@ __device__ __forceinline__ bool run_layer(Smem &S, const __nv_bfloat16 *W, int K
 
 // ---- forward ---------------------------------------------------------------------
 
+// INFER: no pre-activations kept (prediction); the epilogues use the packed forms above.
+template <bool INFER>
 __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     Smem &S = *reinterpret_cast<Smem *>(smem_raw);
@@ -298,25 +368,52 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
         // (a completed MMA has read its input image; the next layer's issue barrier orders
         // this thread's TMEM reads and image writes before the next MMA)
         if (!run_layer(S, W1, 16, phase, a.spin_limit)) break;
-        hidden_epilogue(S.tmem, sb1, S.act, t, zr);
+        if (INFER) hidden_epilogue_infer(S.tmem, sb1, S.act, t);
+        else hidden_epilogue(S.tmem, sb1, S.act, t, zr);
         // layer 2
         if (!run_layer(S, W2, kH, phase, a.spin_limit)) break;
-        hidden_epilogue(S.tmem, sb2, S.act, t, zr ? zr + kH : nullptr);
+        if (INFER) hidden_epilogue_infer(S.tmem, sb2, S.act, t);
+        else hidden_epilogue(S.tmem, sb2, S.act, t, zr ? zr + kH : nullptr);
         // layer 3 and the 64 -> 1 output, 16 columns at a time
         if (!run_layer(S, W3, kH, phase, a.spin_limit)) break;
         float y = 0.0f;
+        if (INFER) {  // pairs: single-precision tanh (the output is not rounded to BF16)
+            const uint64_t half2 = pk2(0.5f, 0.5f);
+            uint64_t yacc = pk2(0.0f, 0.0f);
 #pragma unroll
-        for (int c = 0; c < kH; c += 16) {
-            float z[16];
-            tmem_cols16(S.tmem, c, z);
+            for (int c = 0; c < kH; c += 16) {
+                float z[16];
+                tmem_cols16(S.tmem, c, z);
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                z[i] += sb3[c + i];
-                y += sw4[c + i] * silu(z[i]);
+                for (int i = 0; i < 8; i++) {
+                    const float2 b = *reinterpret_cast<const float2 *>(sb3 + c + 2 * i);
+                    const float2 w = *reinterpret_cast<const float2 *>(sw4 + c + 2 * i);
+                    const uint64_t zz = add2(pk2(z[2 * i], z[2 * i + 1]), pk2(b.x, b.y));
+                    float h0, h1, t0, t1;
+                    upk2(mul2(zz, half2), h0, h1);
+                    asm("tanh.approx.f32 %0, %1;" : "=f"(t0) : "f"(h0));
+                    asm("tanh.approx.f32 %0, %1;" : "=f"(t1) : "f"(h1));
+                    const uint64_t sg = fma2(pk2(t0, t1), half2, half2);
+                    yacc = fma2(pk2(w.x, w.y), mul2(zz, sg), yacc);
+                }
             }
-            if (zr)
+            float y0, y1;
+            upk2(yacc, y0, y1);
+            y = y0 + y1;
+        } else {
 #pragma unroll
-                for (int i = 0; i < 16; i++) zr[2 * kH + c + i] = z[i];
+            for (int c = 0; c < kH; c += 16) {
+                float z[16];
+                tmem_cols16(S.tmem, c, z);
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    z[i] += sb3[c + i];
+                    y += sw4[c + i] * silu(z[i]);
+                }
+                if (zr)
+#pragma unroll
+                    for (int i = 0; i < 16; i++) zr[2 * kH + c + i] = z[i];
+            }
         }
         y += S.vec[4 * kH];
         if (valid) {
@@ -504,8 +601,9 @@ int mlp_pack(const float *params, __nv_bfloat16 *ops, cudaStream_t s) {
 
 int mlp_forward(const MlpForwardArgs &a, int grid, cudaStream_t s) {
     size_t sm = sizeof(Smem);
-    cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_mlp_forward<<<grid, kRows, sm, s>>>(a);
+    auto kern = a.z_out ? k_mlp_forward<false> : k_mlp_forward<true>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<grid, kRows, sm, s>>>(a);
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
 

@@ -50,7 +50,8 @@ struct TileArgs {
     int64_t nrec;
     const double4 *xyz;
     const double *sol;
-    const double *nu_e;
+    const double *nu_e;    // K(nu): per-element reluctivity
+    const double *bscale;  // seeded Jacobian: per-element flux-density scale of the tangent
     QuadParams qp;
     MaterialParams mp;
     double *vals;
@@ -81,8 +82,15 @@ __device__ __forceinline__ double qsum4(double v, const QuadParams &qp, double w
 
 __device__ __forceinline__ void flag(int *err) { atomicOr(err, 1); }
 
-// One element of the block: record i. STIFF: K(nu) with the element's given nu.
-template <bool CALCJ, bool Q4, bool STIFF>
+enum TileMode { kJacobian = 0, kStiffness = 1, kSeeded = 2 };
+
+// One element of the block: record i.
+//   kJacobian: residual and tangent at the element's state (assemble_jacobian_kernel_mex.cpp:92-131);
+//   kStiffness: K(nu) with the element's given nu (assemble_curl_curl_kernel_mex.cpp:94-101), no residual;
+//   kSeeded: residual at B, tangent at the seeded state beta B:
+//            nu(|beta B|^2) Ci.Cj + 2 nu'(|beta B|^2) (beta B.Ci)(beta B.Cj), the operation order of
+//            the two-pass seeded kernel.
+template <bool CALCJ, bool Q4, int MODE>
 __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, double *__restrict__ slot,
                                              double2 *__restrict__ incv, int bnnz, int binc) {
     const int64_t n = A.nrec;
@@ -96,7 +104,9 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
     geometry(A.xyz, tt, g);
     double C[6][3];
     curls_standard(g, C);
+    constexpr bool STIFF = MODE == kStiffness;
     double nu, g2 = 0.0, b[6];
+    double nut = 0.0, be = 1.0;  // seeded tangent: nu(|beta B|^2), beta
     if (STIFF) {
         nu = __ldg(A.nu_e + p2.z);
 #pragma unroll
@@ -119,6 +129,12 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
 #pragma unroll
         for (int j = 0; j < 6; j++) b[j] = dot3(B, C[j]);
         g2 = 2.0 * dnu;
+        if (MODE == kSeeded && CALCJ) {
+            be = __ldg(A.bscale + p2.z);
+            double dnut;
+            material_eval(A.mp, (int)(p2.w & 0xFFu), (be * be) * dot3(B, B), nut, dnut);
+            g2 = 2.0 * dnut;
+        }
     }
     const double adet = g.adet, w0 = A.qp.qw[0] * adet;
 #pragma unroll
@@ -131,7 +147,12 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
         double dv = 0.0;
         if (CALCJ) {
             double v[6];
-            if (g2 == 0.0) {
+            if (MODE == kSeeded) {
+                const double gl = g2 * (be * b[l]);
+#pragma unroll
+                for (int j = 0; j < 6; j++)
+                    v[j] = qsum4<Q4>(nut * dot3(C[l], C[j]) + gl * (be * b[j]), A.qp, w0, adet);
+            } else if (g2 == 0.0) {
 #pragma unroll
                 for (int j = 0; j < 6; j++) v[j] = qsum4<Q4>(nu * dot3(C[l], C[j]), A.qp, w0, adet);
             } else {
@@ -161,8 +182,9 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
     }
 }
 
-template <int BT, int MINB, bool CALCJ, bool Q4, bool STIFF>
+template <int BT, int MINB, bool CALCJ, bool Q4, int MODE>
 __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A) {
+    constexpr bool STIFF = MODE == kStiffness;
     extern __shared__ __align__(16) double tile_smem[];
     const TileBlock *Bp = A.blocks + blockIdx.x;
     const int nrows = Bp->nrows, row0 = Bp->row0, rec0 = Bp->rec0, nrec = Bp->nrec;
@@ -178,13 +200,13 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A) {
         for (int c = 0; c < ncolors; c++) {
             const int c1 = Bp->col_end[c];
             for (int i = c0 + tid; i < c1; i += BT)
-                tile_element<CALCJ, Q4, STIFF>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
+                tile_element<CALCJ, Q4, MODE>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
             c0 = c1;
             __syncthreads();
         }
     } else {
         for (int i = tid; i < nrec; i += BT)
-            tile_element<CALCJ, Q4, STIFF>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
+            tile_element<CALCJ, Q4, MODE>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
         __syncthreads();
     }
     // rows: diagonal and residual in ascending element order
@@ -690,9 +712,9 @@ size_t tile_smem_bytes(const TilePlan &tp, int *smem_nnz) {
     return (size_t)*smem_nnz * sizeof(double) + (size_t)tp.max_inc * sizeof(double2);
 }
 
-template <bool CALCJ, bool Q4, bool STIFF>
+template <bool CALCJ, bool Q4, int MODE>
 int launch(const TileArgs &a, const TilePlan &tp, size_t smem, cudaStream_t s) {
-    auto kern = k_tile<kTileBT, kTileMinB, CALCJ, Q4, STIFF>;
+    auto kern = k_tile<kTileBT, kTileMinB, CALCJ, Q4, MODE>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return MAG_E_CUDA;
     kern<<<tp.nblocks, kTileBT, smem, s>>>(a);
@@ -727,8 +749,9 @@ int launch_tile_jacobian(const TilePlan &tp, const ElemData &m, const double *so
     a.nnz_total = tp.nnz;
     size_t smem = tile_smem_bytes(tp, &a.smem_nnz);
     const bool q4 = qp.nq == 4 && qp.uniform_w;
-    if (calc_j) return q4 ? launch<true, true, false>(a, tp, smem, s) : launch<true, false, false>(a, tp, smem, s);
-    return q4 ? launch<false, true, false>(a, tp, smem, s) : launch<false, false, false>(a, tp, smem, s);
+    if (calc_j)
+        return q4 ? launch<true, true, kJacobian>(a, tp, smem, s) : launch<true, false, kJacobian>(a, tp, smem, s);
+    return q4 ? launch<false, true, kJacobian>(a, tp, smem, s) : launch<false, false, kJacobian>(a, tp, smem, s);
 }
 
 int launch_tile_stiffness(const TilePlan &tp, const ElemData &m, const double *nu, const QuadParams &qp,
@@ -740,7 +763,23 @@ int launch_tile_stiffness(const TilePlan &tp, const ElemData &m, const double *n
     a.nnz_total = tp.nnz;
     size_t smem = tile_smem_bytes(tp, &a.smem_nnz);
     const bool q4 = qp.nq == 4 && qp.uniform_w;
-    return q4 ? launch<true, true, true>(a, tp, smem, s) : launch<true, false, true>(a, tp, smem, s);
+    return q4 ? launch<true, true, kStiffness>(a, tp, smem, s) : launch<true, false, kStiffness>(a, tp, smem, s);
+}
+
+int launch_tile_seeded(const TilePlan &tp, const ElemData &m, const double *sol, const double *bscale,
+                       const QuadParams &qp, const MaterialParams &mp, double *vals, double *res, int *err,
+                       cudaStream_t s) {
+    if (!tp.ok || !qp.standard_curl) return MAG_E_UNSUPPORTED;
+    TileArgs a = make_args(tp, m, qp, err);
+    a.sol = sol;
+    a.bscale = bscale;
+    a.mp = mp;
+    a.vals = vals;
+    a.res = res;
+    a.nnz_total = tp.nnz;
+    size_t smem = tile_smem_bytes(tp, &a.smem_nnz);
+    const bool q4 = qp.nq == 4 && qp.uniform_w;
+    return q4 ? launch<true, true, kSeeded>(a, tp, smem, s) : launch<true, false, kSeeded>(a, tp, smem, s);
 }
 
 }  // namespace mag

@@ -101,6 +101,11 @@ void free_tile_plan(TilePlan *plan);
 int launch_tile_jacobian(const TilePlan &tp, const ElemData &m, const double *sol, const QuadParams &qp,
                          const MaterialParams &mp, int calc_j, double *vals, double *res, int *err,
                          cudaStream_t s);
+// Jacobian with a seeded tangent (mag_assemble_jacobian_seeded): residual at the state,
+// tangent at the flux density scaled by bscale [Ne].
+int launch_tile_seeded(const TilePlan &tp, const ElemData &m, const double *sol, const double *bscale,
+                       const QuadParams &qp, const MaterialParams &mp, double *vals, double *res, int *err,
+                       cudaStream_t s);
 // K(nu) with per-element reluctivity nu [Ne].
 int launch_tile_stiffness(const TilePlan &tp, const ElemData &m, const double *nu, const QuadParams &qp,
                           double *vals, int *err, cudaStream_t s);

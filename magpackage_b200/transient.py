@@ -485,6 +485,10 @@ def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, 
             "ideal": summarize(ideal_rec.stats) if ideal else None,
             "train": {"samples": int(feats.shape[0]), "epochs": epochs, "loss_first": hist[0],
                       "loss_last": hist[-1], "gpu_ms": train_ms},
+            # the whole cost of the learned warm start on steps 101-200: its steps plus the
+            # training on steps 1-100, against the plain warm start's steps
+            "net_gpu_ms": {"plain": summarize(plain2.stats)["gpu_ms"],
+                           "learned_with_training": summarize(learned.stats)["gpu_ms"] + train_ms},
             "per_step": {"plain": [s.newton for s in plain2.stats],
                          "learned": [s.newton for s in learned.stats],
                          "ideal": [s.newton for s in ideal_rec.stats] if ideal else None},

@@ -38,11 +38,20 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+# Where the reference tree is read when the oracle is built: $REF_ROOT, else the
+# read-only mount of the reference in the build container.
+REFERENCE_TREE = os.environ.get("REF_ROOT", "/root/reference")
+
+
 def build(quiet: bool = True) -> None:
-    """Build the oracle libraries (make -C oracle)."""
+    """Build the oracle libraries (make -C oracle); the reference's own kernels too when
+    its tree is present."""
     import subprocess
 
-    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    args = ["make", "-C", HERE]
+    if os.path.isdir(os.path.join(REFERENCE_TREE, "src", "mex")):
+        args.append(f"REF_ROOT={REFERENCE_TREE}")
+    out = subprocess.run(args, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
 
