@@ -539,6 +539,7 @@ def main():
                     choices=sorted(WORKLOADS) + ["batched_complex", "transient", "hbfem", "stiffness", "mex"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--instances", type=int, default=64, help="meshes of the batched_complex workload")
+    ap.add_argument("--tile-variant", type=int, default=None, help="launch shape of the tile Jacobian kernel")
     ap.add_argument("--schedule", default="tile-blocks",
                     choices=["tile-blocks", "shared-row-blocks", "nz-row-blocks", "row-blocks", "two-pass"],
                     help="Jacobian assembly schedule (all give identical bits)")
@@ -593,6 +594,8 @@ def main():
                 "row-blocks": _lib.SCHEDULE_ROW_BLOCKS,
                 "two-pass": _lib.SCHEDULE_TWO_PASS}[args.schedule]
     plan.set_schedule(sched_id)
+    if args.tile_variant is not None:
+        plan.set_tile_variant(args.tile_variant)
     single = sched_id != _lib.SCHEDULE_TWO_PASS
     ne, nnz = mesh.num_elements, plan.nnz
     sol = torch.as_tensor(np.random.default_rng(rank + 1).normal(0.0, 1e-3, E), device="cuda")

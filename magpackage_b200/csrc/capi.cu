@@ -771,6 +771,14 @@ int mag_mesh_set_option(mag_mesh *m, int option, int64_t value) {
         m->schedule = (int)value;
         return MAG_OK;
     }
+    if (option == MAG_OPTION_TILE_VARIANT) {
+        if (value < 0 || value >= kTileVariants) {
+            set_error("tile variant %lld out of range (0..%d)", (long long)value, kTileVariants - 1);
+            return MAG_E_ARG;
+        }
+        m->tile.variant = (int)value;
+        return MAG_OK;
+    }
     set_error("unknown option %d", option);
     return MAG_E_ARG;
 }
@@ -1213,6 +1221,93 @@ int mag_pcg_solve(mag_pcg *p, const int64_t *rp, const int32_t *ci, const double
 
 namespace {
 
+// ---- host <-> device copies of the MEX entry points ---------------------------------
+// The MEX arrays are pageable host memory. cudaMemcpy to or from pageable memory passes
+// through a small driver buffer; a large copy goes faster through two pinned chunks: the
+// DMA of one chunk overlaps the host threads' copy of the other to or from the caller's
+// array (which also touches its pages in parallel).
+constexpr size_t kStageChunk = size_t(32) << 20;
+constexpr size_t kStageMin = size_t(4) << 20;  // smaller copies go direct
+
+struct PinnedStage {
+    void *buf[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool tried = false;
+};
+PinnedStage g_stage;  // used under g_mex_mu
+
+bool stage_ready() {
+    if (!g_stage.tried) {
+        g_stage.tried = true;
+        for (int i = 0; i < 2; i++)
+            if (cudaHostAlloc(&g_stage.buf[i], kStageChunk, cudaHostAllocDefault) != cudaSuccess ||
+                cudaEventCreateWithFlags(&g_stage.ev[i], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                for (int k = 0; k < 2; k++) {
+                    if (g_stage.buf[k]) cudaFreeHost(g_stage.buf[k]);
+                    if (g_stage.ev[k]) cudaEventDestroy(g_stage.ev[k]);
+                    g_stage.buf[k] = nullptr;
+                    g_stage.ev[k] = nullptr;
+                }
+                return false;
+            }
+    }
+    return g_stage.buf[0] != nullptr;
+}
+
+void host_copy(void *dst, const void *src, size_t bytes) {
+    constexpr size_t kPiece = size_t(1) << 20;
+    const int64_t n = (int64_t)((bytes + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < n; k++) {
+        const size_t o = (size_t)k * kPiece, len = bytes - o < kPiece ? bytes - o : kPiece;
+        std::memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o, len);
+    }
+}
+
+// Device -> pageable host, synchronous on return.
+int copy_to_host(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (bytes < kStageMin || !stage_ready()) {
+        MAG_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        MAG_CUDA_TRY(cudaStreamSynchronize(s));
+        return MAG_OK;
+    }
+    const size_t n = (bytes + kStageChunk - 1) / kStageChunk;
+    for (size_t i = 0; i <= n; i++) {
+        if (i < n) {
+            const size_t o = i * kStageChunk, len = bytes - o < kStageChunk ? bytes - o : kStageChunk;
+            MAG_CUDA_TRY(cudaMemcpyAsync(g_stage.buf[i % 2], static_cast<const char *>(src) + o, len,
+                                         cudaMemcpyDeviceToHost, s));
+            MAG_CUDA_TRY(cudaEventRecord(g_stage.ev[i % 2], s));
+        }
+        if (i > 0) {
+            const size_t j = i - 1, o = j * kStageChunk, len = bytes - o < kStageChunk ? bytes - o : kStageChunk;
+            MAG_CUDA_TRY(cudaEventSynchronize(g_stage.ev[j % 2]));
+            host_copy(static_cast<char *>(dst) + o, g_stage.buf[j % 2], len);
+        }
+    }
+    return MAG_OK;
+}
+
+// Pageable host -> device; the source may be reused when this returns.
+int copy_to_device(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (bytes < kStageMin || !stage_ready()) {
+        MAG_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return MAG_OK;
+    }
+    const size_t n = (bytes + kStageChunk - 1) / kStageChunk;
+    for (size_t i = 0; i < n; i++) {
+        const size_t o = i * kStageChunk, len = bytes - o < kStageChunk ? bytes - o : kStageChunk;
+        if (i >= 2) MAG_CUDA_TRY(cudaEventSynchronize(g_stage.ev[i % 2]));  // chunk i-2 has left the buffer
+        host_copy(g_stage.buf[i % 2], static_cast<const char *>(src) + o, len);
+        MAG_CUDA_TRY(cudaMemcpyAsync(static_cast<char *>(dst) + o, g_stage.buf[i % 2], len,
+                                     cudaMemcpyHostToDevice, s));
+        MAG_CUDA_TRY(cudaEventRecord(g_stage.ev[i % 2], s));
+    }
+    for (int k = 0; k < 2; k++) MAG_CUDA_TRY(cudaEventSynchronize(g_stage.ev[k]));
+    return MAG_OK;
+}
+
 // A mesh given in the reference's MEX layout, converted to the device layout. The MEX
 // entry points keep the last kMexCacheEntries of them (per device), keyed by the sizes
 // and a content hash of P, T, Dofs and Signs, so that the Newton loop's calls with the
@@ -1303,10 +1398,10 @@ int mex_convert(const double *P, int64_t Nn, const double *T, int64_t Ne, const 
     MAG_CUDA_TRY(mm.dofs.alloc(Ne * 24));
     MAG_CUDA_TRY(mm.tags.alloc(Ne));
     MAG_CUDA_TRY(mm.signs.alloc(Ne));
-    MAG_CUDA_TRY(cudaMemcpyAsync(Pd.p, P, Nn * 24, cudaMemcpyHostToDevice, s));
-    MAG_CUDA_TRY(cudaMemcpyAsync(Td.p, T, Ne * 32, cudaMemcpyHostToDevice, s));
-    MAG_CUDA_TRY(cudaMemcpyAsync(Dd.p, Dofs, Ne * 48, cudaMemcpyHostToDevice, s));
-    MAG_CUDA_TRY(cudaMemcpyAsync(Sd.p, Signs, Ne * 48, cudaMemcpyHostToDevice, s));
+    MAG_TRY(copy_to_device(Pd.p, P, Nn * 24, s));
+    MAG_TRY(copy_to_device(Td.p, T, Ne * 32, s));
+    MAG_TRY(copy_to_device(Dd.p, Dofs, Ne * 48, s));
+    MAG_TRY(copy_to_device(Sd.p, Signs, Ne * 48, s));
     k_pack_xyz<<<grid(Nn), kB, 0, s>>>(Pd.as<double>(), Nn, mm.xyz.as<double4>(), err.as<int>());
     k_index_from_double<<<grid(4 * Ne), kB, 0, s>>>(Td.as<double>(), 4 * Ne, mm.tet.as<int32_t>(), Nn, 0,
                                                     err.as<int>());
@@ -1334,7 +1429,7 @@ int mex_set_tags(MexMesh &mm, const double *Tags, cudaStream_t s) {
     MAG_CUDA_TRY(Gd.alloc(mm.Ne * 8));
     MAG_CUDA_TRY(cudaMemsetAsync(err.p, 0, 4, s));
     MAG_CUDA_TRY(cudaMemsetAsync(mx.p, 0, 4, s));
-    MAG_CUDA_TRY(cudaMemcpyAsync(Gd.p, Tags, mm.Ne * 8, cudaMemcpyHostToDevice, s));
+    MAG_TRY(copy_to_device(Gd.p, Tags, mm.Ne * 8, s));
     k_pack_tags_f64<<<grid(mm.Ne), kB, 0, s>>>(Gd.as<double>(), mm.Ne, mm.tags.as<uint8_t>(), mx.as<int>(),
                                                err.as<int>());
     int h = 0;
@@ -1427,13 +1522,13 @@ int mex_download(MexMesh &mm, int64_t Ne, int calcj, double *I, double *J, doubl
     MAG_TRY(launch_to_triplets(mm.scratch.as<double>(), mm.dofs.as<int32_t>(), Ne, calcj, dI, dJ, dV,
                                Ridx ? dRi : nullptr, Ridx ? dRv : nullptr, s));
     if (nk) {
-        MAG_CUDA_TRY(cudaMemcpyAsync(I, dI, nk * 8, cudaMemcpyDeviceToHost, s));
-        MAG_CUDA_TRY(cudaMemcpyAsync(J, dJ, nk * 8, cudaMemcpyDeviceToHost, s));
-        MAG_CUDA_TRY(cudaMemcpyAsync(V, dV, nk * 8, cudaMemcpyDeviceToHost, s));
+        MAG_TRY(copy_to_host(I, dI, nk * 8, s));
+        MAG_TRY(copy_to_host(J, dJ, nk * 8, s));
+        MAG_TRY(copy_to_host(V, dV, nk * 8, s));
     }
     if (nr) {
-        MAG_CUDA_TRY(cudaMemcpyAsync(Ridx, dRi, nr * 8, cudaMemcpyDeviceToHost, s));
-        MAG_CUDA_TRY(cudaMemcpyAsync(Rval, dRv, nr * 8, cudaMemcpyDeviceToHost, s));
+        MAG_TRY(copy_to_host(Ridx, dRi, nr * 8, s));
+        MAG_TRY(copy_to_host(Rval, dRv, nr * 8, s));
     }
     MAG_CUDA_TRY(cudaStreamSynchronize(s));
     return MAG_OK;
@@ -1468,7 +1563,7 @@ struct MexJacobian {
         MAG_TRY(make_quad(Qw, nq, CurlRef, CurlRef, &qp, &q, s));
         // dofs must index SolA
         MAG_CUDA_TRY(sol.alloc(Ndof * 8));
-        MAG_CUDA_TRY(cudaMemcpyAsync(sol.p, SolA, Ndof * 8, cudaMemcpyHostToDevice, s));
+        MAG_TRY(copy_to_device(sol.p, SolA, Ndof * 8, s));
         return launch_jacobian_elems(mm->ed, sol.as<double>(), qp, ms.mp, calc_j, mm->scratch.as<double>(), s);
     }
 };
@@ -1719,7 +1814,7 @@ int mex_to_sparse(MexMesh &mm, int64_t Ne, int64_t ndof, bool with_matrix, doubl
     MAG_TRY(launch_rows_reduce(rows, pat.max_row, mm.scratch.as<double>(), with_matrix ? vals.as<double>() : nullptr,
                                h_res ? res.as<double>() : nullptr, s));
     if (h_res) {
-        MAG_CUDA_TRY(cudaMemcpyAsync(h_res, res.p, ndof * 8, cudaMemcpyDeviceToHost, s));
+        MAG_TRY(copy_to_host(h_res, res.p, ndof * 8, s));
         MAG_CUDA_TRY(cudaStreamSynchronize(s));
     }
     if (!with_matrix) return MAG_OK;
@@ -1852,14 +1947,14 @@ int mag_sparse_copy(const mag_sparse *sp, uint64_t *jc, uint64_t *ir, double *pr
     }
     cudaStream_t s = nullptr;
     // column pointers are non-negative: the int64 bits are the mwIndex bits
-    MAG_CUDA_TRY(cudaMemcpyAsync(jc, sp->rp, (sp->n + 1) * 8, cudaMemcpyDeviceToHost, s));
+    std::lock_guard<std::mutex> lk(g_mex_mu);  // the pinned staging buffers
+    MAG_TRY(copy_to_host(jc, sp->rp, (sp->n + 1) * 8, s));
     if (sp->nnz > 0) {
         Dev wide(s);
         MAG_CUDA_TRY(wide.alloc(sp->nnz * 8));
         k_i32_to_u64<<<grid(sp->nnz), kB, 0, s>>>(sp->ci, sp->nnz, wide.as<uint64_t>());
-        MAG_CUDA_TRY(cudaMemcpyAsync(ir, wide.p, sp->nnz * 8, cudaMemcpyDeviceToHost, s));
-        MAG_CUDA_TRY(cudaMemcpyAsync(pr, sp->v, sp->nnz * 8, cudaMemcpyDeviceToHost, s));
-        MAG_CUDA_TRY(cudaStreamSynchronize(s));
+        MAG_TRY(copy_to_host(ir, wide.p, sp->nnz * 8, s));
+        MAG_TRY(copy_to_host(pr, sp->v, sp->nnz * 8, s));
     }
     MAG_CUDA_TRY(cudaStreamSynchronize(s));
     return MAG_OK;

@@ -182,67 +182,91 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
     }
 }
 
+// L2 prefetch of [p, p + bytes) (16-byte aligned start and length; the plan's arrays are
+// padded so that the rounded range stays inside them).
+__device__ __forceinline__ void l2_prefetch(const void *p, size_t bytes) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uintptr_t lo = a & ~uintptr_t(15), hi = (a + bytes + 15) & ~uintptr_t(15);
+    if (hi > lo)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((uint32_t)(hi - lo)) : "memory");
+}
+
+// What a block's next CTA visit will read first: its records (six planes), rows and chunks.
+__device__ __forceinline__ void prefetch_block(const TileArgs &A, int b) {
+    const TileBlock *Bp = A.blocks + b;
+    const int rec0 = Bp->rec0, nrec = Bp->nrec;
+    for (int k = 0; k < 6; k++) l2_prefetch(A.recs + (int64_t)k * A.nrec + rec0, (size_t)nrec * sizeof(uint4));
+    l2_prefetch(A.rows + Bp->row0, (size_t)Bp->nrows * sizeof(uint2));
+    l2_prefetch(A.chunks + Bp->chunk0, (size_t)Bp->nchunks * sizeof(uint2));
+}
+
+// Persistent: CTA c assembles blocks c, c + gridDim.x, ..., and while it works on one it
+// prefetches the records of its next one into L2.
 template <int BT, int MINB, bool CALCJ, bool Q4, int MODE>
-__global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A) {
+__global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks) {
     constexpr bool STIFF = MODE == kStiffness;
     extern __shared__ __align__(16) double tile_smem[];
-    const TileBlock *Bp = A.blocks + blockIdx.x;
-    const int nrows = Bp->nrows, row0 = Bp->row0, rec0 = Bp->rec0, nrec = Bp->nrec;
-    const int nnz = Bp->nnz, ninc = Bp->ninc, ncolors = Bp->ncolors;
-    const int chunk0 = Bp->chunk0, nchunks = Bp->nchunks;
     double *slot = tile_smem;
     double2 *incv = reinterpret_cast<double2 *>(tile_smem + A.smem_nnz);
     const int tid = threadIdx.x;
-    if (CALCJ) {
-        for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
-        __syncthreads();
-        int c0 = 0;
-        for (int c = 0; c < ncolors; c++) {
-            const int c1 = Bp->col_end[c];
-            for (int i = c0 + tid; i < c1; i += BT)
+    for (int blk = blockIdx.x; blk < nblocks; blk += gridDim.x) {
+        if (tid == 0 && blk + (int)gridDim.x < nblocks) prefetch_block(A, blk + gridDim.x);
+        const TileBlock *Bp = A.blocks + blk;
+        const int nrows = Bp->nrows, row0 = Bp->row0, rec0 = Bp->rec0, nrec = Bp->nrec;
+        const int nnz = Bp->nnz, ninc = Bp->ninc, ncolors = Bp->ncolors;
+        const int chunk0 = Bp->chunk0, nchunks = Bp->nchunks;
+        if (CALCJ) {
+            for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
+            __syncthreads();
+            int c0 = 0;
+            for (int c = 0; c < ncolors; c++) {
+                const int c1 = Bp->col_end[c];
+                for (int i = c0 + tid; i < c1; i += BT)
+                    tile_element<CALCJ, Q4, MODE>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
+                c0 = c1;
+                __syncthreads();
+            }
+        } else {
+            for (int i = tid; i < nrec; i += BT)
                 tile_element<CALCJ, Q4, MODE>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
-            c0 = c1;
             __syncthreads();
         }
-    } else {
-        for (int i = tid; i < nrec; i += BT)
-            tile_element<CALCJ, Q4, MODE>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
-        __syncthreads();
-    }
-    // rows: diagonal and residual in ascending element order
-    for (int r = tid; r < nrows; r += BT) {
-        const uint2 rw = __ldg(A.rows + row0 + r);
-        const int nzb = (int)(rw.y & 0x1FFFu), incb = (int)((rw.y >> 13) & 0xFFFu);
-        const int diag = (int)((rw.y >> 25) & 31u);
-        int ince = r + 1 < nrows ? (int)((__ldg(&A.rows[row0 + r + 1].y) >> 13) & 0xFFFu) : ninc;
-        if (ince > ninc) ince = ninc;
-        double racc = 0.0, dacc = 0.0;
-        for (int k = incb; k < ince; k++) {
-            const double2 v = incv[k];
-            racc = racc + v.x;
-            if (CALCJ) dacc = dacc + v.y;
-        }
-        if (!STIFF) {
-            if ((int64_t)rw.x < A.ndof) A.res[rw.x] = racc;
-            else flag(A.err);
-        }
-        if (CALCJ && ince > incb) {
-            if (nzb + diag < nnz) slot[nzb + diag] = dacc;
-            else flag(A.err);
-        }
-    }
-    if (CALCJ) {
-        __syncthreads();
-        const int warp = tid >> 5, lane = tid & 31;
-        for (int c = warp; c < nchunks; c += BT / 32) {
-            const uint2 ch = __ldg(A.chunks + chunk0 + c);
-            const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
-            const int64_t g = (int64_t)ch.y;
-            if (sb0 + len > nnz || g + len > A.nnz_total) {
-                if (lane == 0) flag(A.err);
-                continue;
+        // rows: diagonal and residual in ascending element order
+        for (int r = tid; r < nrows; r += BT) {
+            const uint2 rw = __ldg(A.rows + row0 + r);
+            const int nzb = (int)(rw.y & 0x1FFFu), incb = (int)((rw.y >> 13) & 0xFFFu);
+            const int diag = (int)((rw.y >> 25) & 31u);
+            int ince = r + 1 < nrows ? (int)((__ldg(&A.rows[row0 + r + 1].y) >> 13) & 0xFFFu) : ninc;
+            if (ince > ninc) ince = ninc;
+            double racc = 0.0, dacc = 0.0;
+            for (int k = incb; k < ince; k++) {
+                const double2 v = incv[k];
+                racc = racc + v.x;
+                if (CALCJ) dacc = dacc + v.y;
             }
-            for (int i = lane; i < len; i += 32) A.vals[g + i] = slot[sb0 + i];
+            if (!STIFF) {
+                if ((int64_t)rw.x < A.ndof) A.res[rw.x] = racc;
+                else flag(A.err);
+            }
+            if (CALCJ && ince > incb) {
+                if (nzb + diag < nnz) slot[nzb + diag] = dacc;
+                else flag(A.err);
+            }
+        }
+        __syncthreads();
+        if (CALCJ) {
+            const int warp = tid >> 5, lane = tid & 31;
+            for (int c = warp; c < nchunks; c += BT / 32) {
+                const uint2 ch = __ldg(A.chunks + chunk0 + c);
+                const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
+                const int64_t g = (int64_t)ch.y;
+                if (sb0 + len > nnz || g + len > A.nnz_total) {
+                    if (lane == 0) flag(A.err);
+                    continue;
+                }
+                for (int i = lane; i < len; i += 32) A.vals[g + i] = slot[sb0 + i];
+            }
+            __syncthreads();  // the next block zeroes the slots these stores read
         }
     }
 }
@@ -683,8 +707,9 @@ int build_tile_plan(const TilePlanInput &in, TilePlan *plan, cudaStream_t s) {
     p.max_inc = hp.max_inc;
     p.max_colors = hp.max_colors;
     p.evals_per_elem = (double)nrec / (double)in.ne;
-    const size_t b_blk = (size_t)nb * sizeof(TileBlock), b_rows = hp.rows.size() * sizeof(uint2),
-                 b_ch = (size_t)std::max<int64_t>(nch, 1) * sizeof(uint2),
+    // rows and chunks padded by 16 bytes: the kernel's L2 prefetches round to 16 bytes
+    const size_t b_blk = (size_t)nb * sizeof(TileBlock), b_rows = hp.rows.size() * sizeof(uint2) + 16,
+                 b_ch = (size_t)std::max<int64_t>(nch, 1) * sizeof(uint2) + 16,
                  b_rec = (size_t)std::max<int64_t>(6 * nrec, 1) * sizeof(uint4);
     if (cudaMalloc(&p.blocks, b_blk) != cudaSuccess || cudaMalloc(&p.rows, b_rows) != cudaSuccess ||
         cudaMalloc(&p.chunks, b_ch) != cudaSuccess || cudaMalloc(&p.recs, b_rec) != cudaSuccess) {
@@ -693,7 +718,7 @@ int build_tile_plan(const TilePlanInput &in, TilePlan *plan, cudaStream_t s) {
         return MAG_OK;  // no room: the other schedules remain
     }
     MAG_CUDA_TRY(cudaMemcpyAsync(p.blocks, hp.blocks.data(), b_blk, cudaMemcpyHostToDevice, s));
-    MAG_CUDA_TRY(cudaMemcpyAsync(p.rows, hp.rows.data(), b_rows, cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(p.rows, hp.rows.data(), hp.rows.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
     if (nch) MAG_CUDA_TRY(cudaMemcpyAsync(p.chunks, hp.chunks.data(), nch * sizeof(uint2), cudaMemcpyHostToDevice, s));
     if (nrec)
         MAG_CUDA_TRY(cudaMemcpyAsync(p.recs, hp.planes.data(), 6 * nrec * sizeof(uint4), cudaMemcpyHostToDevice, s));
@@ -712,12 +737,19 @@ size_t tile_smem_bytes(const TilePlan &tp, int *smem_nnz) {
     return (size_t)*smem_nnz * sizeof(double) + (size_t)tp.max_inc * sizeof(double2);
 }
 
-template <bool CALCJ, bool Q4, int MODE>
+template <bool CALCJ, bool Q4, int MODE, int BT = kTileBT, int MINB = kTileMinB>
 int launch(const TileArgs &a, const TilePlan &tp, size_t smem, cudaStream_t s) {
-    auto kern = k_tile<kTileBT, kTileMinB, CALCJ, Q4, MODE>;
+    auto kern = k_tile<BT, MINB, CALCJ, Q4, MODE>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return MAG_E_CUDA;
-    kern<<<tp.nblocks, kTileBT, smem, s>>>(a);
+    // one persistent CTA per resident slot
+    int dev = 0, nsm = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, BT, smem) != cudaSuccess || per < 1)
+        return MAG_E_CUDA;
+    const int grid = tp.nblocks < per * nsm ? tp.nblocks : per * nsm;
+    kern<<<grid, BT, smem, s>>>(a, tp.nblocks);
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
 
@@ -749,9 +781,22 @@ int launch_tile_jacobian(const TilePlan &tp, const ElemData &m, const double *so
     a.nnz_total = tp.nnz;
     size_t smem = tile_smem_bytes(tp, &a.smem_nnz);
     const bool q4 = qp.nq == 4 && qp.uniform_w;
-    if (calc_j)
-        return q4 ? launch<true, true, kJacobian>(a, tp, smem, s) : launch<true, false, kJacobian>(a, tp, smem, s);
+    if (calc_j && q4) {  // the launch shape of the Newton Jacobian (threads per CTA x CTAs per SM)
+        switch (tp.variant) {
+            case 1: return launch<true, true, kJacobian, 288, 2>(a, tp, smem, s);
+            case 2: return launch<true, true, kJacobian, 320, 2>(a, tp, smem, s);
+            case 3: return launch<true, true, kJacobian, 512, 1>(a, tp, smem, s);
+            default: return launch<true, true, kJacobian>(a, tp, smem, s);
+        }
+    }
+    if (calc_j) return launch<true, false, kJacobian>(a, tp, smem, s);
     return q4 ? launch<false, true, kJacobian>(a, tp, smem, s) : launch<false, false, kJacobian>(a, tp, smem, s);
+}
+
+const char *tile_variant_name(int v) {
+    static const char *names[kTileVariants] = {"256 threads x 2 CTAs/SM", "288 threads x 2 CTAs/SM",
+                                               "320 threads x 2 CTAs/SM", "512 threads x 1 CTA/SM"};
+    return v >= 0 && v < kTileVariants ? names[v] : "";
 }
 
 int launch_tile_stiffness(const TilePlan &tp, const ElemData &m, const double *nu, const QuadParams &qp,

@@ -14,6 +14,7 @@ constexpr int kTileMaxNnz = 8191;   // CSR nonzeros per block (13-bit offsets in
 constexpr int kTileMaxInc = 4095;   // (row, element) incidences per block (12-bit offsets)
 constexpr int kTileMaxColors = 8;   // element colour classes per block
 constexpr int kTileChunk = 256;     // nonzeros per store chunk (one warp stores a chunk)
+constexpr int kTileVariants = 4;    // launch shapes of the Jacobian kernel (tile_variant_name)
 constexpr uint32_t kTileAbsent = 0xFFFFFFFFu;
 
 // One CTA's work: whole CSR rows whose edges start in one spatial tile of nodes, and
@@ -54,6 +55,7 @@ struct TilePlan {
     double build_ms = 0.0;
     int64_t bytes = 0;
     int ok = 0;
+    int variant = 0;  // launch shape of the Newton Jacobian (0 .. kTileVariants-1)
 };
 
 struct TilePlanInput {
@@ -106,6 +108,7 @@ int launch_tile_jacobian(const TilePlan &tp, const ElemData &m, const double *so
 int launch_tile_seeded(const TilePlan &tp, const ElemData &m, const double *sol, const double *bscale,
                        const QuadParams &qp, const MaterialParams &mp, double *vals, double *res, int *err,
                        cudaStream_t s);
+const char *tile_variant_name(int v);
 // K(nu) with per-element reluctivity nu [Ne].
 int launch_tile_stiffness(const TilePlan &tp, const ElemData &m, const double *nu, const QuadParams &qp,
                           double *vals, int *err, cudaStream_t s);

@@ -78,6 +78,10 @@ class AssemblyPlan:
         _lib.check(self._lib.mag_mesh_get_info(self._h, C.byref(info)))
         self.info = info
 
+    def set_tile_variant(self, variant: int):
+        """Launch shape of the tile schedule's Jacobian kernel (MAG_OPTION_TILE_VARIANT)."""
+        _lib.check(self._lib.mag_mesh_set_option(self._h, 2, int(variant)))
+
     def check(self, stream=None):
         """Synchronise and raise if a bounded device-side wait gave up."""
         _lib.check(self._lib.mag_mesh_check(self._h, _lib.stream_ptr(stream)))

@@ -638,6 +638,14 @@ def test_tile_schedule_shuffled_numbering_and_unused_dofs(oracle_port):
     v2, r2 = plan.jacobian(x)
     assert torch.equal(v.view(torch.int64), v2.view(torch.int64)) and torch.equal(r.view(torch.int64),
                                                                                    r2.view(torch.int64))
+    for variant in (1, 2, 3, 0):  # every launch shape gives the same bits
+        plan.set_tile_variant(variant)
+        v3, r3 = plan.jacobian(x)
+        plan.check()
+        assert torch.equal(v.view(torch.int64), v3.view(torch.int64)), variant
+        assert torch.equal(r.view(torch.int64), r3.view(torch.int64)), variant
+    with pytest.raises(_lib.MagError):
+        plan.set_tile_variant(4)
     nu = np.random.default_rng(5).uniform(0.2, 5.0, T.shape[0]) * material.NU0
     Ik, Jk, Vk = oracle_port.curl_curl(m, nu, qw, curl)
     assert_csr_equal(plan.row_ptr, plan.col_idx, plan.stiffness(dev(nu)), oracle_matrix(oracle_port, Ik, Jk, Vk, n, False))
