@@ -64,8 +64,8 @@ typedef struct {
 
 /* Jacobian assembly schedules; all give identical bits. */
 #define MAG_OPTION_SCHEDULE 1
-#define MAG_OPTION_TILE_VARIANT 2 /* launch shape of the tile schedule's Jacobian kernel: 0 = 256 threads x
-                                     2 CTAs/SM (default), 1 = 288 x 2, 2 = 320 x 2, 3 = 512 x 1; same bits */
+#define MAG_OPTION_TILE_VARIANT 2 /* launch shape of the tile schedule's Jacobian kernel: 0 = 320 threads x
+                                     2 CTAs/SM (default), 1 = 288 x 2, 2 = 256 x 2, 3 = 512 x 1; same bits */
 #define MAG_SCHEDULE_TWO_PASS 0   /* element kernel + row reduction through an HBM scratch slab */
 #define MAG_SCHEDULE_RETIRED_1 1  /* retired (a persistent launch over an L2 scratch ring); rejected */
 #define MAG_SCHEDULE_ROW_BLOCKS 2 /* one launch, no scratch: per-row element recompute */

@@ -20,7 +20,11 @@ __device__ __forceinline__ unsigned derived_signs(int4 t) {
     return b;
 }
 
-__device__ __forceinline__ double flip(double v, unsigned neg) { return neg ? -v : v; }
+// -v when neg is set: negation is a flip of the sign bit, done here as one integer XOR of
+// the high word instead of a select between v and -v.
+__device__ __forceinline__ double flip(double v, unsigned neg) {
+    return __longlong_as_double(__double_as_longlong(v) ^ ((long long)(neg & 1u) << 63));
+}
 
 struct Geo {
     double J[3][3];

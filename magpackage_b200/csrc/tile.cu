@@ -200,17 +200,18 @@ __device__ __forceinline__ void prefetch_block(const TileArgs &A, int b) {
     l2_prefetch(A.chunks + Bp->chunk0, (size_t)Bp->nchunks * sizeof(uint2));
 }
 
-// Persistent: CTA c assembles blocks c, c + gridDim.x, ..., and while it works on one it
-// prefetches the records of its next one into L2.
+// One CTA per block. The CTA of block b prefetches into L2 the records of block b + ahead
+// (ahead = the CTAs resident at once), the block the hardware starts about when b ends.
 template <int BT, int MINB, bool CALCJ, bool Q4, int MODE>
-__global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks) {
+__global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int ahead) {
     constexpr bool STIFF = MODE == kStiffness;
     extern __shared__ __align__(16) double tile_smem[];
     double *slot = tile_smem;
     double2 *incv = reinterpret_cast<double2 *>(tile_smem + A.smem_nnz);
     const int tid = threadIdx.x;
-    for (int blk = blockIdx.x; blk < nblocks; blk += gridDim.x) {
-        if (tid == 0 && blk + (int)gridDim.x < nblocks) prefetch_block(A, blk + gridDim.x);
+    {
+        const int blk = blockIdx.x;
+        if (tid == 0 && blk + ahead < nblocks) prefetch_block(A, blk + ahead);
         const TileBlock *Bp = A.blocks + blk;
         const int nrows = Bp->nrows, row0 = Bp->row0, rec0 = Bp->rec0, nrec = Bp->nrec;
         const int nnz = Bp->nnz, ninc = Bp->ninc, ncolors = Bp->ncolors;
@@ -266,12 +267,13 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks) {
                 }
                 for (int i = lane; i < len; i += 32) A.vals[g + i] = slot[sb0 + i];
             }
-            __syncthreads();  // the next block zeroes the slots these stores read
         }
     }
 }
 
-constexpr int kTileBT = 256;
+// 320 threads: a colour class of an interior 4x4x4 tile holds about 288 elements, so each
+// colour phase runs in one pass (256 threads left a second pass with one warp busy).
+constexpr int kTileBT = 320;
 constexpr int kTileMinB = 2;
 
 // ---- host plan builder --------------------------------------------------------------
@@ -742,14 +744,13 @@ int launch(const TileArgs &a, const TilePlan &tp, size_t smem, cudaStream_t s) {
     auto kern = k_tile<BT, MINB, CALCJ, Q4, MODE>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return MAG_E_CUDA;
-    // one persistent CTA per resident slot
+    // CTAs resident at once: how far ahead a CTA prefetches
     int dev = 0, nsm = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, BT, smem) != cudaSuccess || per < 1)
         return MAG_E_CUDA;
-    const int grid = tp.nblocks < per * nsm ? tp.nblocks : per * nsm;
-    kern<<<grid, BT, smem, s>>>(a, tp.nblocks);
+    kern<<<tp.nblocks, BT, smem, s>>>(a, tp.nblocks, per * nsm);
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
 
@@ -784,7 +785,7 @@ int launch_tile_jacobian(const TilePlan &tp, const ElemData &m, const double *so
     if (calc_j && q4) {  // the launch shape of the Newton Jacobian (threads per CTA x CTAs per SM)
         switch (tp.variant) {
             case 1: return launch<true, true, kJacobian, 288, 2>(a, tp, smem, s);
-            case 2: return launch<true, true, kJacobian, 320, 2>(a, tp, smem, s);
+            case 2: return launch<true, true, kJacobian, 256, 2>(a, tp, smem, s);
             case 3: return launch<true, true, kJacobian, 512, 1>(a, tp, smem, s);
             default: return launch<true, true, kJacobian>(a, tp, smem, s);
         }
@@ -794,8 +795,8 @@ int launch_tile_jacobian(const TilePlan &tp, const ElemData &m, const double *so
 }
 
 const char *tile_variant_name(int v) {
-    static const char *names[kTileVariants] = {"256 threads x 2 CTAs/SM", "288 threads x 2 CTAs/SM",
-                                               "320 threads x 2 CTAs/SM", "512 threads x 1 CTA/SM"};
+    static const char *names[kTileVariants] = {"320 threads x 2 CTAs/SM", "288 threads x 2 CTAs/SM",
+                                               "256 threads x 2 CTAs/SM", "512 threads x 1 CTA/SM"};
     return v >= 0 && v < kTileVariants ? names[v] : "";
 }
 
