@@ -36,6 +36,11 @@
 #include "element.cuh"
 #include "tile.cuh"
 
+// Node layers per tile along z (x and y: 4); a build option (-DMAG_TILE_LAYERS_Z=n).
+#ifndef MAG_TILE_LAYERS_Z
+#define MAG_TILE_LAYERS_Z 4
+#endif
+
 namespace mag {
 
 namespace {
@@ -84,21 +89,6 @@ __device__ __forceinline__ void flag(int *err) { atomicOr(err, 1); }
 
 enum TileMode { kJacobian = 0, kStiffness = 1, kSeeded = 2 };
 
-// The 16-bit plan entry of (row l, column j != l) from the record's planes 4-7.
-__device__ __forceinline__ unsigned entry_of(const uint32_t ew[16], int l, int j) {
-    const int idx = l * 5 + (j < l ? j : j - 1);
-    return (ew[idx >> 1] >> ((idx & 1) * 16)) & 0xFFFFu;
-}
-
-// Off-diagonal entry into its slot of the block's values (entry as above). A slot index
-// has 13 bits and the slot region holds kTileSlotCap values, so any index stays inside
-// this CTA's shared memory.
-__device__ __forceinline__ void put_entry(double *__restrict__ slot, unsigned e, double v) {
-    if (e == 0xFFFFu) return;
-    const unsigned k = e & 0x1FFFu;
-    slot[k] = slot[k] + flip(v, (e >> 13) & 1u);
-}
-
 // One element of the block: record i.
 //   kJacobian: residual and tangent at the element's state (assemble_jacobian_kernel_mex.cpp:92-131);
 //   kStiffness: K(nu) with the element's given nu (assemble_curl_curl_kernel_mex.cpp:94-101), no residual;
@@ -111,14 +101,10 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
     const int64_t n = A.nrec;
     const uint4 p0 = __ldg(A.recs + i), p1 = __ldg(A.recs + n + i), p2 = __ldg(A.recs + 2 * n + i);
     const uint4 p3 = __ldg(A.recs + 3 * n + i), p4 = __ldg(A.recs + 4 * n + i), p5 = __ldg(A.recs + 5 * n + i);
-    const uint4 p6 = __ldg(A.recs + 6 * n + i), p7 = __ldg(A.recs + 7 * n + i);
     const int4 tt = make_int4((int)p0.x, (int)p0.y, (int)p0.z, (int)p0.w);
     const unsigned sb = (p2.w >> 8) & 0x3Fu;
-    const uint32_t isw[3] = {p3.x, p3.y, p3.z};
-    const uint32_t ew[16] = {p4.x, p4.y, p4.z, p4.w, p5.x, p5.y, p5.z, p5.w,
-                             p6.x, p6.y, p6.z, p6.w, p7.x, p7.y, p7.z, p7.w};
-    // incidence slot of local row l, 0xFFFF when the row is not one of the block's
-    auto inc_slot = [&](int l) { return (isw[l >> 1] >> ((l & 1) * 16)) & 0xFFFFu; };
+    const unsigned pos[6] = {p3.x, p3.y, p3.z, p3.w, p4.x, p4.y};
+    const unsigned sl[6] = {p4.z, p4.w, p5.x, p5.y, p5.z, p5.w};
     Geo g;
     geometry(A.xyz, tt, g);
     double C[6][3];
@@ -156,15 +142,16 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
         }
     }
     const double adet = g.adet, w0 = A.qp.qw[0] * adet;
-    // per present row: its tangent row, each off-diagonal entry placed as soon as it is
-    // formed, and its residual and diagonal entry into its incidence slot
 #pragma unroll
     for (int l = 0; l < 6; l++) {
-        const unsigned is = inc_slot(l);
-        if (is == 0xFFFFu) continue;
-        const double rv = STIFF ? 0.0 : flip(qsum4<Q4>(nu * b[l], A.qp, w0, adet), (sb >> l) & 1u);
+        const unsigned s = sl[l];
+        if (s == kTileAbsent) continue;
+        const int nzb = (int)(s & 0xFFFFu), is = (int)(s >> 16);
+        const unsigned si = (sb >> l) & 1u;
+        const double rv = STIFF ? 0.0 : flip(qsum4<Q4>(nu * b[l], A.qp, w0, adet), si);
         double dv = 0.0;
         if (CALCJ) {
+            // each entry placed as soon as it is formed (few live registers)
             const double gl = MODE == kSeeded ? g2 * (be * b[l]) : g2 * b[l];
 #pragma unroll
             for (int j = 0; j < 6; j++) {
@@ -172,12 +159,22 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
                 if (MODE == kSeeded) v = qsum4<Q4>(nut * dot3(C[l], C[j]) + gl * (be * b[j]), A.qp, w0, adet);
                 else if (g2 == 0.0) v = qsum4<Q4>(nu * dot3(C[l], C[j]), A.qp, w0, adet);
                 else v = qsum4<Q4>(nu * dot3(C[l], C[j]) + gl * b[j], A.qp, w0, adet);
-                if (j == l) dv = v;  // the diagonal: s_l ^ s_l = 0, no flip
-                else put_entry(slot, entry_of(ew, l, j), v);
+                if (j == l) {
+                    dv = v;  // the diagonal: si ^ si = 0, no flip
+                    continue;
+                }
+                const unsigned p = (pos[l] >> (5 * j)) & 31u;
+                if (p == (unsigned)kCompactMaxRow) continue;
+                const int k = nzb + (int)p;
+                if (k < bnnz) slot[k] = slot[k] + flip(v, si ^ ((sb >> j) & 1u));
+                else flag(A.err);
             }
         }
-        if ((int)is < binc) incv[is] = make_double2(rv, dv);
-        else flag(A.err);
+        if (is < binc) {
+            incv[is] = make_double2(rv, dv);
+        } else {
+            flag(A.err);
+        }
     }
 }
 
@@ -277,41 +274,9 @@ constexpr int kTileMinB = 2;
 
 // ---- host plan builder --------------------------------------------------------------
 
-// A record while the block is planned: tet, dofs, element id, tag | sign bits << 8
-// (words 0-11, the first three planes as stored), then per local row its six 5-bit
-// in-row positions (words 12-17) and its slot word (nonzero base | incidence slot << 16,
-// or kTileAbsent; words 18-23). encode_record turns the last two into the stored form.
 struct HostRec {
-    uint32_t w[24];
+    uint32_t w[24];  // the six 16-byte planes of one record, plane-major
 };
-
-// The stored record (kTileRecPlanes 16-byte planes): planes 0-2 as HostRec words 0-11;
-// plane 3: the incidence slot of each local row, 16 bits each (0xFFFF = row not in the
-// block); planes 4-7: for each local row l and column j != l (entry l * 5 + (j < l ? j :
-// j - 1)) the entry's slot in the block's values (13 bits) and whether it is negated
-// (s_l xor s_j, bit 13), or 0xFFFF (no entry: row absent or column without a dof).
-void encode_record(const HostRec &h, uint32_t out[4 * kTileRecPlanes]) {
-    for (int i = 0; i < 12; i++) out[i] = h.w[i];
-    const unsigned sb = (h.w[11] >> 8) & 0x3Fu;
-    uint16_t is[8] = {0xFFFF, 0xFFFF, 0xFFFF, 0xFFFF, 0xFFFF, 0xFFFF, 0xFFFF, 0xFFFF};
-    uint16_t ent[32];
-    for (int i = 0; i < 32; i++) ent[i] = 0xFFFF;
-    for (int l = 0; l < 6; l++) {
-        const uint32_t sl = h.w[18 + l];
-        if (sl == kTileAbsent) continue;
-        is[l] = (uint16_t)(sl >> 16);
-        const uint32_t nzb = sl & 0xFFFFu;
-        for (int j = 0, c = 0; j < 6; j++) {
-            if (j == l) continue;
-            const uint32_t p = (h.w[12 + l] >> (5 * j)) & 31u;
-            if (p != (uint32_t)kCompactMaxRow)
-                ent[l * 5 + c] = (uint16_t)((nzb + p) | ((((sb >> l) ^ (sb >> j)) & 1u) << 13));
-            c++;
-        }
-    }
-    for (int i = 0; i < 4; i++) out[12 + i] = (uint32_t)is[2 * i] | ((uint32_t)is[2 * i + 1] << 16);
-    for (int i = 0; i < 16; i++) out[16 + i] = (uint32_t)ent[2 * i] | ((uint32_t)ent[2 * i + 1] << 16);
-}
 
 // Layer index of every node along one axis: sorted coordinates split where
 // consecutive values are more than 0.3 h apart or a layer would span more than h.
@@ -390,12 +355,12 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
     if (!(h > 0.0)) h = 1.0;
     std::vector<int32_t> layer[3];
     for (int a = 0; a < 3; a++) axis_layers(xyz, a, h, layer[a]);
-    constexpr int kTileLayers = 4;
+    constexpr int kTileLayers[3] = {4, 4, MAG_TILE_LAYERS_Z};
     int32_t ntile[3] = {1, 1, 1};
     for (int a = 0; a < 3; a++) {
         int32_t m = 0;
         for (int32_t v : layer[a]) m = std::max(m, v);
-        ntile[a] = m / kTileLayers + 1;
+        ntile[a] = m / kTileLayers[a] + 1;
     }
     const int64_t tiles = (int64_t)ntile[0] * ntile[1] * ntile[2];
     if (tiles >= (int64_t(1) << 31)) return false;
@@ -412,8 +377,8 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
                 const int *t = &tet[e].x;
                 const int32_t na = t[edge_a(l)], nb = t[edge_b(l)];
                 const int32_t node = na < nb ? na : nb;
-                prev = (layer[0][node] / kTileLayers) +
-                       ntile[0] * ((layer[1][node] / kTileLayers) + ntile[1] * (layer[2][node] / kTileLayers));
+                prev = (layer[0][node] / kTileLayers[0]) +
+                       ntile[0] * ((layer[1][node] / kTileLayers[1]) + ntile[1] * (layer[2][node] / kTileLayers[2]));
             }
             row_tile[r] = prev;
         }
@@ -648,10 +613,19 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
                     continue;
                 }
             }
-            // records by colour, ascending element within a colour
+            // records by colour; within a colour by the set of the element's rows in the block
+            // (most rows first), so that the threads of a warp run the same rows
             std::vector<int32_t> idx((size_t)nr);
-            for (int32_t i = 0; i < nr; i++) idx[i] = i;
-            std::stable_sort(idx.begin(), idx.end(), [&](int32_t x, int32_t y) { return color[x] < color[y]; });
+            std::vector<uint32_t> rkey((size_t)nr);
+            for (int32_t i = 0; i < nr; i++) {
+                idx[i] = i;
+                uint32_t m = 0;
+                for (int l = 0; l < 6; l++) m |= (rec[i].w[18 + l] != kTileAbsent ? 1u : 0u) << l;
+                rkey[i] = ((6u - (uint32_t)__builtin_popcount(m)) << 6) | m;
+            }
+            std::stable_sort(idx.begin(), idx.end(), [&](int32_t x, int32_t y) {
+                return color[x] != color[y] ? color[x] < color[y] : rkey[x] < rkey[y];
+            });
             std::vector<HostRec> sorted((size_t)nr);
             for (int32_t i = 0; i < nr; i++) sorted[i] = rec[idx[i]];
             rec.swap(sorted);
@@ -677,26 +651,29 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
         max_col = std::max(max_col, blocks[b].ncolors);
         if (nrec >= (int64_t(1) << 31) || nch >= (int64_t(1) << 31)) return false;
     }
-    std::vector<uint4> planes((size_t)(kTileRecPlanes * nrec));
+    std::vector<uint4> planes((size_t)(6 * nrec));
     std::vector<uint2> chunks((size_t)nch);
-    std::atomic<int64_t> present{0};
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t b = 0; b < nb; b++) {
         const std::vector<HostRec> &rec = brec[b];
         const int64_t o = blocks[b].rec0;
-        int64_t here = 0;
-        for (size_t i = 0; i < rec.size(); i++) {
-            uint32_t w[4 * kTileRecPlanes];
-            encode_record(rec[i], w);
-            for (int k = 0; k < kTileRecPlanes; k++)
-                planes[(size_t)k * nrec + o + i] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
-            for (int l = 0; l < 6; l++) here += rec[i].w[18 + l] != kTileAbsent;
-        }
-        present += here;
+        for (size_t i = 0; i < rec.size(); i++)
+            for (int k = 0; k < 6; k++) {
+                const uint32_t *w = rec[i].w + 4 * k;
+                planes[(size_t)k * nrec + o + i] = make_uint4(w[0], w[1], w[2], w[3]);
+            }
         std::copy(bchunk[b].begin(), bchunk[b].end(), chunks.begin() + blocks[b].chunk0);
     }
     // coverage check: every incidence is one record slot
-    if (present.load() != ninc_total) return false;
+    {
+        int64_t present = 0;
+        for (int64_t i = 0; i < nrec; i++) {
+            const uint4 a = planes[4 * nrec + i], c = planes[5 * nrec + i];
+            const uint32_t sl[6] = {a.z, a.w, c.x, c.y, c.z, c.w};
+            for (int l = 0; l < 6; l++) present += sl[l] != kTileAbsent;
+        }
+        if (present != ninc_total) return false;
+    }
     out->blocks.swap(blocks);
     out->rows.swap(rows);
     out->chunks.swap(chunks);
@@ -740,7 +717,7 @@ int build_tile_plan(const TilePlanInput &in, TilePlan *plan, cudaStream_t s) {
     // rows and chunks padded by 16 bytes: the kernel's L2 prefetches round to 16 bytes
     const size_t b_blk = (size_t)nb * sizeof(TileBlock), b_rows = hp.rows.size() * sizeof(uint2) + 16,
                  b_ch = (size_t)std::max<int64_t>(nch, 1) * sizeof(uint2) + 16,
-                 b_rec = (size_t)std::max<int64_t>(kTileRecPlanes * nrec, 1) * sizeof(uint4);
+                 b_rec = (size_t)std::max<int64_t>(6 * nrec, 1) * sizeof(uint4);
     if (cudaMalloc(&p.blocks, b_blk) != cudaSuccess || cudaMalloc(&p.rows, b_rows) != cudaSuccess ||
         cudaMalloc(&p.chunks, b_ch) != cudaSuccess || cudaMalloc(&p.recs, b_rec) != cudaSuccess) {
         free_tile_plan(&p);
@@ -751,8 +728,7 @@ int build_tile_plan(const TilePlanInput &in, TilePlan *plan, cudaStream_t s) {
     MAG_CUDA_TRY(cudaMemcpyAsync(p.rows, hp.rows.data(), hp.rows.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
     if (nch) MAG_CUDA_TRY(cudaMemcpyAsync(p.chunks, hp.chunks.data(), nch * sizeof(uint2), cudaMemcpyHostToDevice, s));
     if (nrec)
-        MAG_CUDA_TRY(cudaMemcpyAsync(p.recs, hp.planes.data(), kTileRecPlanes * nrec * sizeof(uint4),
-                                     cudaMemcpyHostToDevice, s));
+        MAG_CUDA_TRY(cudaMemcpyAsync(p.recs, hp.planes.data(), 6 * nrec * sizeof(uint4), cudaMemcpyHostToDevice, s));
     MAG_CUDA_TRY(cudaStreamSynchronize(s));
     p.bytes = (int64_t)(b_blk + b_rows + b_ch + b_rec);
     p.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
@@ -764,7 +740,7 @@ int build_tile_plan(const TilePlanInput &in, TilePlan *plan, cudaStream_t s) {
 namespace {
 
 size_t tile_smem_bytes(const TilePlan &tp, int *smem_nnz) {
-    *smem_nnz = kTileSlotCap;  // every 13-bit slot index of a plan entry lands inside the region
+    *smem_nnz = (tp.max_nnz + 1) & ~1;
     return (size_t)*smem_nnz * sizeof(double) + (size_t)tp.max_inc * sizeof(double2);
 }
 

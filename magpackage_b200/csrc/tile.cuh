@@ -30,18 +30,16 @@ struct TileBlock {
 };
 static_assert(sizeof(TileBlock) == 80, "TileBlock layout");
 
-constexpr int kTileRecPlanes = 8;   // 16-byte planes of a record
-constexpr int kTileSlotCap = 8192;  // shared-memory value slots: every 13-bit slot index
-
-// Device plan. Records are 128 bytes in eight 16-byte planes (plane k of record i at
+// Device plan. Records are 96 bytes in six 16-byte planes (plane k of record i at
 // recs[k * nrec_total + i]) so that a warp's loads of one plane are contiguous:
 //   plane 0: tet (4 node ids)
 //   plane 1: dofs 0..3
 //   plane 2: dofs 4, 5, element id, tag | sign bits << 8
-//   plane 3: per local row its incidence slot (16 bits; 0xFFFF = row not in the block)
-//   planes 4-7: per local row l and column j != l (entry l * 5 + (j < l ? j : j - 1), 16
-//            bits each) the entry's slot in the block's values | negated << 13, or
-//            0xFFFF (no entry)
+//   plane 3: per local row 0..3 its six 5-bit in-row column positions (31 = no dof)
+//   plane 4: positions of local rows 4, 5; slots of local rows 0, 1
+//   plane 5: slots of local rows 2..5
+// where a slot is (row's first nonzero in the block) | (incidence slot << 16), or
+// kTileAbsent when the row is not one of the block's.
 // rows: per block row (ascending ids) x = global row, y = nonzero base (13 bits) |
 // incidence base (12 bits) << 13 | diagonal position (5 bits) << 25.
 // chunks: x = block nonzero base | length << 16, y = global nonzero base.
