@@ -40,6 +40,14 @@
 #ifndef MAG_TILE_LAYERS_Z
 #define MAG_TILE_LAYERS_Z 4
 #endif
+// Order a colour's records by the rows they hold in the block (build option).
+#ifndef MAG_TILE_SORT_ROWS
+#define MAG_TILE_SORT_ROWS 1
+#endif
+// Load a row's off-diagonal slots together before updating them (build option).
+#ifndef MAG_TILE_BATCH_LOADS
+#define MAG_TILE_BATCH_LOADS 0
+#endif
 
 namespace mag {
 
@@ -64,6 +72,7 @@ struct TileArgs {
     int *err;
     int64_t nnz_total, ndof;
     int smem_nnz;  // doubles reserved for the block's values (even)
+    int smem_inc, smem_rows, smem_chunks;  // incidence slots, row-table and chunk entries reserved
 };
 
 // Sum over the quadrature points of v * w_q (w_q = qw_q |det J|) from zero, in point
@@ -151,8 +160,19 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
         const double rv = STIFF ? 0.0 : flip(qsum4<Q4>(nu * b[l], A.qp, w0, adet), si);
         double dv = 0.0;
         if (CALCJ) {
-            // each entry placed as soon as it is formed (few live registers)
             const double gl = MODE == kSeeded ? g2 * (be * b[l]) : g2 * b[l];
+#if MAG_TILE_BATCH_LOADS
+            // The row's five off-diagonal slots are distinct nonzeros: their current values
+            // are loaded together first, so the loads overlap instead of each waiting for
+            // the previous entry's store.
+            double o[6];
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                const unsigned p = (pos[l] >> (5 * j)) & 31u;
+                const int k = nzb + (int)p;
+                o[j] = (j != l && p != (unsigned)kCompactMaxRow && k < bnnz) ? slot[k] : 0.0;
+            }
+#endif
 #pragma unroll
             for (int j = 0; j < 6; j++) {
                 double v;
@@ -166,7 +186,11 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
                 const unsigned p = (pos[l] >> (5 * j)) & 31u;
                 if (p == (unsigned)kCompactMaxRow) continue;
                 const int k = nzb + (int)p;
+#if MAG_TILE_BATCH_LOADS
+                if (k < bnnz) slot[k] = o[j] + flip(v, si ^ ((sb >> j) & 1u));
+#else
                 if (k < bnnz) slot[k] = slot[k] + flip(v, si ^ ((sb >> j) & 1u));
+#endif
                 else flag(A.err);
             }
         }
@@ -196,14 +220,26 @@ __device__ __forceinline__ void prefetch_block(const TileArgs &A, int b) {
     l2_prefetch(A.chunks + Bp->chunk0, (size_t)Bp->nchunks * sizeof(uint2));
 }
 
+// 8-byte asynchronous global -> shared copies (both addresses 8-byte aligned).
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // One CTA per block. The CTA of block b prefetches into L2 the records of block b + ahead
 // (ahead = the CTAs resident at once), the block the hardware starts about when b ends.
+// The block's row table and store chunks are copied into shared memory while its
+// elements run, so the row and store phases start without a global round trip.
 template <int BT, int MINB, bool CALCJ, bool Q4, int MODE>
 __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int ahead) {
     constexpr bool STIFF = MODE == kStiffness;
     extern __shared__ __align__(16) double tile_smem[];
     double *slot = tile_smem;
     double2 *incv = reinterpret_cast<double2 *>(tile_smem + A.smem_nnz);
+    uint2 *srows = reinterpret_cast<uint2 *>(incv + A.smem_inc);
+    uint2 *schunks = srows + A.smem_rows;
     const int tid = threadIdx.x;
     {
         const int blk = blockIdx.x;
@@ -212,6 +248,14 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int 
         const int nrows = Bp->nrows, row0 = Bp->row0, rec0 = Bp->rec0, nrec = Bp->nrec;
         const int nnz = Bp->nnz, ninc = Bp->ninc, ncolors = Bp->ncolors;
         const int chunk0 = Bp->chunk0, nchunks = Bp->nchunks;
+        if (nrows > A.smem_rows || nchunks > A.smem_chunks || nnz > A.smem_nnz || ninc > A.smem_inc) {
+            if (tid == 0) flag(A.err);  // the whole CTA leaves before its first barrier
+            return;
+        }
+        for (int i = tid; i < nrows; i += BT) cp_async8(srows + i, A.rows + row0 + i);
+        if (CALCJ)
+            for (int i = tid; i < nchunks; i += BT) cp_async8(schunks + i, A.chunks + chunk0 + i);
+        cp_async_commit();
         if (CALCJ) {
             for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
             __syncthreads();
@@ -221,19 +265,25 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int 
                 for (int i = c0 + tid; i < c1; i += BT)
                     tile_element<CALCJ, Q4, MODE>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
                 c0 = c1;
+                if (c + 1 == ncolors) cp_async_wait_all();
+                __syncthreads();
+            }
+            if (ncolors == 0) {
+                cp_async_wait_all();
                 __syncthreads();
             }
         } else {
             for (int i = tid; i < nrec; i += BT)
                 tile_element<CALCJ, Q4, MODE>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
+            cp_async_wait_all();
             __syncthreads();
         }
         // rows: diagonal and residual in ascending element order
         for (int r = tid; r < nrows; r += BT) {
-            const uint2 rw = __ldg(A.rows + row0 + r);
+            const uint2 rw = srows[r];
             const int nzb = (int)(rw.y & 0x1FFFu), incb = (int)((rw.y >> 13) & 0xFFFu);
             const int diag = (int)((rw.y >> 25) & 31u);
-            int ince = r + 1 < nrows ? (int)((__ldg(&A.rows[row0 + r + 1].y) >> 13) & 0xFFFu) : ninc;
+            int ince = r + 1 < nrows ? (int)((srows[r + 1].y >> 13) & 0xFFFu) : ninc;
             if (ince > ninc) ince = ninc;
             double racc = 0.0, dacc = 0.0;
             for (int k = incb; k < ince; k++) {
@@ -254,7 +304,7 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int 
         if (CALCJ) {
             const int warp = tid >> 5, lane = tid & 31;
             for (int c = warp; c < nchunks; c += BT / 32) {
-                const uint2 ch = __ldg(A.chunks + chunk0 + c);
+                const uint2 ch = schunks[c];
                 const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
                 const int64_t g = (int64_t)ch.y;
                 if (sb0 + len > nnz || g + len > A.nnz_total) {
@@ -613,15 +663,18 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
                     continue;
                 }
             }
-            // records by colour; within a colour by the set of the element's rows in the block
-            // (most rows first), so that the threads of a warp run the same rows
+            // records by colour; within a colour in ascending element order, or (build option)
+            // by the set of the element's rows in the block, most rows first, so that the
+            // threads of a warp run the same rows
             std::vector<int32_t> idx((size_t)nr);
-            std::vector<uint32_t> rkey((size_t)nr);
+            std::vector<uint32_t> rkey((size_t)nr, 0u);
             for (int32_t i = 0; i < nr; i++) {
                 idx[i] = i;
-                uint32_t m = 0;
-                for (int l = 0; l < 6; l++) m |= (rec[i].w[18 + l] != kTileAbsent ? 1u : 0u) << l;
-                rkey[i] = ((6u - (uint32_t)__builtin_popcount(m)) << 6) | m;
+                if (MAG_TILE_SORT_ROWS) {
+                    uint32_t m = 0;
+                    for (int l = 0; l < 6; l++) m |= (rec[i].w[18 + l] != kTileAbsent ? 1u : 0u) << l;
+                    rkey[i] = ((6u - (uint32_t)__builtin_popcount(m)) << 6) | m;
+                }
             }
             std::stable_sort(idx.begin(), idx.end(), [&](int32_t x, int32_t y) {
                 return color[x] != color[y] ? color[x] < color[y] : rkey[x] < rkey[y];
@@ -640,7 +693,7 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
 
     // concatenate: record and chunk offsets, planes
     int64_t nrec = 0, nch = 0;
-    int32_t max_nnz = 0, max_inc = 0, max_col = 0;
+    int32_t max_nnz = 0, max_inc = 0, max_col = 0, max_rows = 0, max_ch = 0;
     for (int64_t b = 0; b < nb; b++) {
         blocks[b].rec0 = (int32_t)nrec;
         blocks[b].chunk0 = (int32_t)nch;
@@ -649,6 +702,8 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
         max_nnz = std::max(max_nnz, blocks[b].nnz);
         max_inc = std::max(max_inc, blocks[b].ninc);
         max_col = std::max(max_col, blocks[b].ncolors);
+        max_rows = std::max(max_rows, blocks[b].nrows);
+        max_ch = std::max(max_ch, blocks[b].nchunks);
         if (nrec >= (int64_t(1) << 31) || nch >= (int64_t(1) << 31)) return false;
     }
     std::vector<uint4> planes((size_t)(6 * nrec));
@@ -682,6 +737,8 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
     out->max_nnz = max_nnz;
     out->max_inc = max_inc;
     out->max_colors = max_col;
+    out->max_rows = max_rows;
+    out->max_chunks = max_ch;
     return true;
 }
 
@@ -713,6 +770,8 @@ int build_tile_plan(const TilePlanInput &in, TilePlan *plan, cudaStream_t s) {
     p.max_nnz = hp.max_nnz;
     p.max_inc = hp.max_inc;
     p.max_colors = hp.max_colors;
+    p.max_rows = hp.max_rows;
+    p.max_chunks = hp.max_chunks;
     p.evals_per_elem = (double)nrec / (double)in.ne;
     // rows and chunks padded by 16 bytes: the kernel's L2 prefetches round to 16 bytes
     const size_t b_blk = (size_t)nb * sizeof(TileBlock), b_rows = hp.rows.size() * sizeof(uint2) + 16,
@@ -739,9 +798,15 @@ int build_tile_plan(const TilePlanInput &in, TilePlan *plan, cudaStream_t s) {
 
 namespace {
 
-size_t tile_smem_bytes(const TilePlan &tp, int *smem_nnz) {
-    *smem_nnz = (tp.max_nnz + 1) & ~1;
-    return (size_t)*smem_nnz * sizeof(double) + (size_t)tp.max_inc * sizeof(double2);
+// Shared memory of one CTA: the block's values (an even count of doubles), the incidence
+// slots (double2), then the block's row table and store chunks (uint2 each).
+size_t tile_smem_bytes(const TilePlan &tp, TileArgs *a) {
+    a->smem_nnz = (tp.max_nnz + 1) & ~1;
+    a->smem_inc = tp.max_inc;
+    a->smem_rows = tp.max_rows;
+    a->smem_chunks = tp.max_chunks;
+    return (size_t)a->smem_nnz * sizeof(double) + (size_t)a->smem_inc * sizeof(double2) +
+           (size_t)(a->smem_rows + a->smem_chunks) * sizeof(uint2);
 }
 
 template <bool CALCJ, bool Q4, int MODE, int BT = kTileBT, int MINB = kTileMinB>
@@ -785,7 +850,7 @@ int launch_tile_jacobian(const TilePlan &tp, const ElemData &m, const double *so
     a.vals = vals;
     a.res = res;
     a.nnz_total = tp.nnz;
-    size_t smem = tile_smem_bytes(tp, &a.smem_nnz);
+    size_t smem = tile_smem_bytes(tp, &a);
     const bool q4 = qp.nq == 4 && qp.uniform_w;
     if (calc_j && q4) {  // the launch shape of the Newton Jacobian (threads per CTA x CTAs per SM)
         switch (tp.variant) {
@@ -812,7 +877,7 @@ int launch_tile_stiffness(const TilePlan &tp, const ElemData &m, const double *n
     a.nu_e = nu;
     a.vals = vals;
     a.nnz_total = tp.nnz;
-    size_t smem = tile_smem_bytes(tp, &a.smem_nnz);
+    size_t smem = tile_smem_bytes(tp, &a);
     const bool q4 = qp.nq == 4 && qp.uniform_w;
     return q4 ? launch<true, true, kStiffness>(a, tp, smem, s) : launch<true, false, kStiffness>(a, tp, smem, s);
 }
@@ -828,7 +893,7 @@ int launch_tile_seeded(const TilePlan &tp, const ElemData &m, const double *sol,
     a.vals = vals;
     a.res = res;
     a.nnz_total = tp.nnz;
-    size_t smem = tile_smem_bytes(tp, &a.smem_nnz);
+    size_t smem = tile_smem_bytes(tp, &a);
     const bool q4 = qp.nq == 4 && qp.uniform_w;
     return q4 ? launch<true, true, kSeeded>(a, tp, smem, s) : launch<true, false, kSeeded>(a, tp, smem, s);
 }

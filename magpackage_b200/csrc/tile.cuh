@@ -50,7 +50,7 @@ struct TilePlan {
     uint4 *recs = nullptr;
     int32_t nblocks = 0;
     int64_t nrows = 0, nchunks = 0, nrec = 0, nnz = 0;
-    int32_t max_nnz = 0, max_inc = 0, max_colors = 0;
+    int32_t max_nnz = 0, max_inc = 0, max_colors = 0, max_rows = 0, max_chunks = 0;
     double evals_per_elem = 0.0;  // records / elements
     double build_ms = 0.0;
     int64_t bytes = 0;
@@ -86,7 +86,7 @@ struct TileHostPlan {
     std::vector<uint2> rows, chunks;
     std::vector<uint4> planes;  // 6 * nrec
     int64_t nrec = 0;
-    int32_t max_nnz = 0, max_inc = 0, max_colors = 0;
+    int32_t max_nnz = 0, max_inc = 0, max_colors = 0, max_rows = 0, max_chunks = 0;
 };
 
 // The planner itself (host only): false when the mesh does not suit the schedule.
