@@ -339,12 +339,33 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
     const __nv_bfloat16 *W1 = S.w, *W2 = S.w + kW1pElems, *W3 = S.w + kW1pElems + kWElems;
     const float *sb1 = S.vec, *sb2 = S.vec + kH, *sb3 = S.vec + 2 * kH, *sw4 = S.vec + 3 * kH;
     uint32_t phase = 0;
+    // The next tile's feature row (one 16-byte load: feature rows are 16 bytes, the buffer
+    // 16-byte aligned) and output index are loaded one tile ahead, so their DRAM latency
+    // overlaps the current tile's layers.
+    const float4 *feats4 = reinterpret_cast<const float4 *>(a.feats);
+    float4 f_next = make_float4(0.f, 0.f, 0.f, 0.f);
+    int64_t dst_next = 0;
+    {
+        const int64_t r0 = (int64_t)blockIdx.x * kRows + t;
+        if (r0 < a.n) {
+            f_next = __ldg(feats4 + r0);
+            dst_next = a.rows ? (int64_t)__ldg(a.rows + r0) : r0;
+        }
+    }
     for (int tile = blockIdx.x; tile * kRows < a.n; tile += gridDim.x) {
         const int64_t row = (int64_t)tile * kRows + t;
         const bool valid = row < a.n;
+        const float4 f = f_next;
+        const int64_t dst = dst_next;
+        {
+            const int64_t rn = row + (int64_t)gridDim.x * kRows;
+            if (rn < a.n) {
+                f_next = __ldg(feats4 + rn);
+                dst_next = a.rows ? (int64_t)__ldg(a.rows + rn) : rn;
+            }
+        }
         float x[4] = {0, 0, 0, 0};
-        if (valid) {  // one 16-byte load per row (feature rows are 16 bytes, the buffer 16-byte aligned)
-            const float4 f = __ldg(reinterpret_cast<const float4 *>(a.feats) + row);
+        if (valid) {
             x[0] = f.x;
             x[1] = f.y;
             x[2] = f.z;
@@ -414,7 +435,7 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
             if (a.nu_out) {  // nu = exp(y * scale + shift), clamped to [nu_min, nu_max]
                 double v = exp((double)y * a.y_scale + a.y_shift);
                 v = v < a.nu_min ? a.nu_min : (v > a.nu_max ? a.nu_max : v);
-                a.nu_out[a.rows ? a.rows[row] : row] = v;
+                a.nu_out[dst] = v;
             }
         }
         tc_fence_before();

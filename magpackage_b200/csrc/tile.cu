@@ -42,11 +42,7 @@
 #endif
 // Order a colour's records by the rows they hold in the block (build option).
 #ifndef MAG_TILE_SORT_ROWS
-#define MAG_TILE_SORT_ROWS 1
-#endif
-// Load a row's off-diagonal slots together before updating them (build option).
-#ifndef MAG_TILE_BATCH_LOADS
-#define MAG_TILE_BATCH_LOADS 0
+#define MAG_TILE_SORT_ROWS 0
 #endif
 
 namespace mag {
@@ -160,37 +156,31 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
         const double rv = STIFF ? 0.0 : flip(qsum4<Q4>(nu * b[l], A.qp, w0, adet), si);
         double dv = 0.0;
         if (CALCJ) {
-            const double gl = MODE == kSeeded ? g2 * (be * b[l]) : g2 * b[l];
-#if MAG_TILE_BATCH_LOADS
-            // The row's five off-diagonal slots are distinct nonzeros: their current values
-            // are loaded together first, so the loads overlap instead of each waiting for
-            // the previous entry's store.
-            double o[6];
+            // the row's six entries first, then its five off-diagonal updates (the six
+            // independent chains of arithmetic overlap; placing each entry as it is formed
+            // measured slower)
+            double v[6];
+            if (MODE == kSeeded) {
+                const double gl = g2 * (be * b[l]);
 #pragma unroll
-            for (int j = 0; j < 6; j++) {
-                const unsigned p = (pos[l] >> (5 * j)) & 31u;
-                const int k = nzb + (int)p;
-                o[j] = (j != l && p != (unsigned)kCompactMaxRow && k < bnnz) ? slot[k] : 0.0;
+                for (int j = 0; j < 6; j++)
+                    v[j] = qsum4<Q4>(nut * dot3(C[l], C[j]) + gl * (be * b[j]), A.qp, w0, adet);
+            } else if (g2 == 0.0) {
+#pragma unroll
+                for (int j = 0; j < 6; j++) v[j] = qsum4<Q4>(nu * dot3(C[l], C[j]), A.qp, w0, adet);
+            } else {
+                const double gl = g2 * b[l];
+#pragma unroll
+                for (int j = 0; j < 6; j++) v[j] = qsum4<Q4>(nu * dot3(C[l], C[j]) + gl * b[j], A.qp, w0, adet);
             }
-#endif
+            dv = v[l];  // the diagonal: si ^ si = 0, no flip
 #pragma unroll
             for (int j = 0; j < 6; j++) {
-                double v;
-                if (MODE == kSeeded) v = qsum4<Q4>(nut * dot3(C[l], C[j]) + gl * (be * b[j]), A.qp, w0, adet);
-                else if (g2 == 0.0) v = qsum4<Q4>(nu * dot3(C[l], C[j]), A.qp, w0, adet);
-                else v = qsum4<Q4>(nu * dot3(C[l], C[j]) + gl * b[j], A.qp, w0, adet);
-                if (j == l) {
-                    dv = v;  // the diagonal: si ^ si = 0, no flip
-                    continue;
-                }
+                if (j == l) continue;
                 const unsigned p = (pos[l] >> (5 * j)) & 31u;
                 if (p == (unsigned)kCompactMaxRow) continue;
                 const int k = nzb + (int)p;
-#if MAG_TILE_BATCH_LOADS
-                if (k < bnnz) slot[k] = o[j] + flip(v, si ^ ((sb >> j) & 1u));
-#else
-                if (k < bnnz) slot[k] = slot[k] + flip(v, si ^ ((sb >> j) & 1u));
-#endif
+                if (k < bnnz) slot[k] = slot[k] + flip(v[j], si ^ ((sb >> j) & 1u));
                 else flag(A.err);
             }
         }
