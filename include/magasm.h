@@ -226,12 +226,15 @@ typedef struct mag_batch mag_batch;
 
 /* A_i = K_i(nu_i) + j*omega_i*M_i(sigma_i) for n independent meshes, the system
  * FrequencySolver.solve forms (src/solver/FrequencySolver.m:87,125,131) without
- * its regularisation term, assembled in ONE persistent launch over a work queue
- * of (mesh, row block) items. d_nu[i] and d_sigma[i] are per-element device
- * arrays (d_sigma[i] may be NULL: sigma = 1); d_vals[i] receives complex128
- * values (re, im interleaved) on mesh i's structural pattern; omega in rad/s.
- * Creation times every compiled variant (incidences per CTA x CTAs per SM) on
- * these inputs, keeps the fastest, and captures its launch in a CUDA graph. */
+ * its regularisation term, assembled in ONE launch over a work queue of
+ * (mesh, block) items: variants 0-3 take the meshes' row blocks (persistent CTAs;
+ * incidences per CTA x CTAs per SM), variants 4-5 their tile blocks (one CTA per
+ * item; threads per CTA), available when every mesh has a tile plan. d_nu[i] and
+ * d_sigma[i] are per-element device arrays (d_sigma[i] may be NULL: sigma = 1);
+ * d_vals[i] receives complex128 values (re, im interleaved) on mesh i's
+ * structural pattern; omega in rad/s. Creation times every available variant on
+ * these inputs, keeps the fastest, and captures its launch in a CUDA graph.
+ * Every variant gives the same bits. */
 int mag_batch_create(mag_mesh *const *meshes, int n, const double *const *d_nu,
                      const double *const *d_sigma, const double *omega, double *const *d_vals,
                      mag_batch **out, void *stream);

@@ -18,8 +18,11 @@
 //              way the pair is (K_ab, omega * M_ab): exactly what MATLAB forms for
 //              K + 1j*omega*M from the two assembled matrices
 //              (FrequencySolver.m:131), where 0*M adds nothing to the real part.
-// The launch is captured once in a CUDA graph and replayed. Block size and CTA
-// residency are chosen per batch by timing the candidates (mag_batch_create).
+// Variants 4 and 5 run the same assembly on the meshes' tile blocks instead
+// (k_tile_complex in tile.cu: one evaluation of each element per block it touches, K
+// pass then M pass). The launch is captured once in a CUDA graph and replayed. The
+// variant (schedule, block size, CTA residency) is chosen per batch by timing every
+// available one (mag_batch_create).
 #include <algorithm>
 #include <vector>
 
@@ -314,10 +317,18 @@ int batch_build(BatchState *b, cudaStream_t s) {
         d.grid = std::max(1, std::min(d.nitems, nsm * std::max(per, 1)));
     }
     MAG_CUDA_TRY(cudaStreamSynchronize(s));
-    return MAG_OK;
+    // the tile-block variants, when every mesh has a tile plan
+    return build_tile_complex(b->tile_in, &b->tile, s);
 }
 
 int batch_launch(const BatchState &b, int variant, cudaStream_t s) {
+    if (variant >= kNumVariants) {
+        if (launch_tile_complex(b.tile, variant - kNumVariants, s) != MAG_OK) {
+            set_error("batch launch (tile blocks): %s", cudaGetErrorString(cudaGetLastError()));
+            return MAG_E_CUDA;
+        }
+        return MAG_OK;
+    }
     const BatchVariantData &d = b.var[variant];
     const Variant &v = kVariants[variant];
     v.fn<<<d.grid, v.threads, v.smem, s>>>(static_cast<const BatchInstance *>(d.inst),
@@ -330,12 +341,18 @@ int batch_launch(const BatchState &b, int variant, cudaStream_t s) {
     return MAG_OK;
 }
 
-int batch_num_variants() { return kNumVariants; }
-bool batch_variant_available(const BatchState &b, int v) { return v >= 0 && v < kNumVariants && b.var[v].nitems > 0; }
-const char *batch_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : ""; }
-int batch_variant_threads(int v) { return kVariants[v].threads; }
+int batch_num_variants() { return kNumVariants + kTileComplexVariants; }
+bool batch_variant_available(const BatchState &b, int v) {
+    if (v >= kNumVariants) return v < kNumVariants + kTileComplexVariants && b.tile.ok;
+    return v >= 0 && b.var[v].nitems > 0;
+}
+const char *batch_variant_name(int v) {
+    if (v >= kNumVariants) return tile_complex_variant_name(v - kNumVariants);
+    return v >= 0 ? kVariants[v].name : "";
+}
 
 void batch_free_variants(BatchState *b) {
+    free_tile_complex(&b->tile);
     for (auto &d : b->var) {
         if (d.items) cudaFree(d.items);
         if (d.inst) cudaFree(d.inst);

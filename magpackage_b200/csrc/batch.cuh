@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "tile.cuh"
 
 namespace mag {
 
@@ -39,6 +40,8 @@ struct BatchState {
     std::vector<int32_t> nblocks256, nblocks128;
     std::vector<int32_t *> owned;  // block_row128 arrays built for the batch
     BatchVariantData var[4];
+    std::vector<TileComplexInput> tile_in;  // the meshes' tile plans (variants 4, 5)
+    TileComplexBatch tile;
 };
 
 int batch_build(BatchState *b, cudaStream_t s);
@@ -46,7 +49,6 @@ int batch_launch(const BatchState &b, int variant, cudaStream_t s);
 int batch_num_variants();
 bool batch_variant_available(const BatchState &b, int v);
 const char *batch_variant_name(int v);
-int batch_variant_threads(int v);
 void batch_free_variants(BatchState *b);
 
 }  // namespace mag

@@ -901,6 +901,8 @@ int mag_batch_create(mag_mesh *const *meshes, int n, const double *const *d_nu, 
         bi.omega = omega[i];
         bi.vals = d_vals[i];
         b->st.inst_host.push_back(bi);
+        b->st.tile_in.push_back(TileComplexInput{&m->tile, m->elems(), m->qp, d_nu[i], bi.sigma, omega[i],
+                                                 d_vals[i], m->status});
         b->st.inst_ne.push_back(m->ne);
         b->st.block_row256.push_back(m->rowblock.block_row);
         b->st.nblocks256.push_back(m->rowblock.nblocks);

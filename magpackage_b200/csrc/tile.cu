@@ -307,6 +307,193 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int 
     }
 }
 
+// ---- batched complex assembly: K(nu) + j omega M(sigma) over many meshes ------------
+
+struct TileComplexInstance {
+    TileArgs a;              // the mesh's plan, coordinates, nu (nu_e), quadrature, error word
+    const double *sigma;     // [Ne] or NULL (sigma = 1)
+    const double *val_ref;   // [18 * nq] reference basis values, entry (i, c, q) at i + 6c + 18q
+    double omega;
+    double *cvals;           // complex128 [nnz] as (re, im)
+};
+
+// The sigma-mass rows of one element of the block (assemble_mass_kernel_mex.cpp:186-230):
+// per local row l, m_j = sum_q ((N_l . N_j) sigma) w_q with N = J^{-T} N_ref at each point,
+// signed; off-diagonal entries into their nonzeros' slots, the diagonal into the
+// incidence slot's x. Elements with |sigma| <= 1e-12 add nothing (the reference skips
+// them; a skipped contribution and a +0 one give the same sums).
+__device__ __forceinline__ void tile_mass_element(const TileComplexInstance &I, int64_t i, double *__restrict__ slot,
+                                                  double2 *__restrict__ incv, int bnnz, int binc,
+                                                  const double *__restrict__ sval) {
+    const TileArgs &A = I.a;
+    const int64_t n = A.nrec;
+    const uint4 p2 = __ldg(A.recs + 2 * n + i);
+    const double sigma = I.sigma ? __ldg(I.sigma + p2.z) : 1.0;
+    if (!(fabs(sigma) > 1e-12)) return;
+    const uint4 p0 = __ldg(A.recs + i), p3 = __ldg(A.recs + 3 * n + i), p4 = __ldg(A.recs + 4 * n + i),
+                p5 = __ldg(A.recs + 5 * n + i);
+    const int4 tt = make_int4((int)p0.x, (int)p0.y, (int)p0.z, (int)p0.w);
+    const unsigned sb = (p2.w >> 8) & 0x3Fu;
+    const unsigned pos[6] = {p3.x, p3.y, p3.z, p3.w, p4.x, p4.y};
+    const unsigned sl[6] = {p4.z, p4.w, p5.x, p5.y, p5.z, p5.w};
+    Geo g;
+    geometry(A.xyz, tt, g);
+    double iv[3][3];
+    inverse3(g, iv);
+    const int nq = A.qp.nq;
+#pragma unroll
+    for (int l = 0; l < 6; l++) {
+        const unsigned s = sl[l];
+        if (s == kTileAbsent) continue;
+        const int nzb = (int)(s & 0xFFFFu), is = (int)(s >> 16);
+        const unsigned si = (sb >> l) & 1u;
+        double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+        for (int q = 0; q < nq; q++) {
+            const double w = A.qp.qw[q] * g.adet;
+            const double *r = sval + 18 * q;
+            double Nl[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) Nl[c] = iv[0][c] * r[l] + iv[1][c] * r[l + 6] + iv[2][c] * r[l + 12];
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                double Nj[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) Nj[c] = iv[0][c] * r[j] + iv[1][c] * r[j + 6] + iv[2][c] * r[j + 12];
+                m[j] = m[j] + dot3(Nl, Nj) * sigma * w;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            if (j == l) continue;
+            const unsigned p = (pos[l] >> (5 * j)) & 31u;
+            if (p == (unsigned)kCompactMaxRow) continue;
+            const int k = nzb + (int)p;
+            if (k < bnnz) slot[k] = slot[k] + flip(m[j], si ^ ((sb >> j) & 1u));
+            else flag(A.err);
+        }
+        if (is < binc) incv[is].x = m[l];  // the diagonal: si ^ si = 0, no flip
+        else flag(A.err);
+    }
+}
+
+// Sums each row's diagonal contributions (incidence slots, component x or y) in ascending
+// element order into the row's diagonal nonzero.
+template <int BT, bool COMP_Y>
+__device__ __forceinline__ void tile_rows_diag(const uint2 *srows, int nrows, const double2 *incv, int ninc,
+                                               double *slot, int nnz, int *err) {
+    for (int r = threadIdx.x; r < nrows; r += BT) {
+        const uint2 rw = srows[r];
+        const int nzb = (int)(rw.y & 0x1FFFu), incb = (int)((rw.y >> 13) & 0xFFFu);
+        const int diag = (int)((rw.y >> 25) & 31u);
+        int ince = r + 1 < nrows ? (int)((srows[r + 1].y >> 13) & 0xFFFu) : ninc;
+        if (ince > ninc) ince = ninc;
+        double dacc = 0.0;
+        for (int k = incb; k < ince; k++) dacc = dacc + (COMP_Y ? incv[k].y : incv[k].x);
+        if (ince > incb) {
+            if (nzb + diag < nnz) slot[nzb + diag] = dacc;
+            else flag(err);
+        }
+    }
+}
+
+// One CTA per (mesh, block) item. K pass: the tile kernel's K(nu) elements (incidence
+// slots get (0, K diagonal)), row sums, real parts stored. M pass, only when some element
+// of the block conducts: slots zeroed again, the conducting elements' M rows, row sums,
+// imaginary parts stored as omega * M; otherwise the imaginary parts are omega * 0.
+// Values equal (K_ab, omega * M_ab) of MATLAB's K + 1j*omega*M (FrequencySolver.m:131).
+template <int BT, int MINB, bool Q4>
+__global__ void __launch_bounds__(BT, MINB)
+    k_tile_complex(const TileComplexInstance *__restrict__ inst, const int2 *__restrict__ items, int nitems,
+                   int ahead, int smem_nnz, int smem_inc, int smem_rows, int smem_chunks) {
+    extern __shared__ __align__(16) double tile_smem[];
+    double *slot = tile_smem;
+    double2 *incv = reinterpret_cast<double2 *>(tile_smem + smem_nnz);
+    uint2 *srows = reinterpret_cast<uint2 *>(incv + smem_inc);
+    uint2 *schunks = srows + smem_rows;
+    double *sval = reinterpret_cast<double *>(schunks + smem_chunks);
+    const int tid = threadIdx.x;
+    const int it = blockIdx.x;
+    if (tid == 0 && it + ahead < nitems) {
+        const int2 nx = items[it + ahead];
+        prefetch_block(inst[nx.x].a, nx.y);
+    }
+    const int2 w = items[it];
+    const TileComplexInstance &I = inst[w.x];
+    const TileArgs &A = I.a;
+    const TileBlock *Bp = A.blocks + w.y;
+    const int nrows = Bp->nrows, row0 = Bp->row0, rec0 = Bp->rec0;
+    const int nnz = Bp->nnz, ninc = Bp->ninc, ncolors = Bp->ncolors;
+    const int chunk0 = Bp->chunk0, nchunks = Bp->nchunks;
+    const int nq = A.qp.nq;
+    if (nrows > smem_rows || nchunks > smem_chunks || nnz > smem_nnz || ninc > smem_inc || nq > kMaxQuad) {
+        if (tid == 0) flag(A.err);  // the whole CTA leaves before its first barrier
+        return;
+    }
+    for (int i = tid; i < nrows; i += BT) cp_async8(srows + i, A.rows + row0 + i);
+    for (int i = tid; i < nchunks; i += BT) cp_async8(schunks + i, A.chunks + chunk0 + i);
+    cp_async_commit();
+    for (int i = tid; i < 18 * nq; i += BT) sval[i] = __ldg(I.val_ref + i);
+    for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
+    __syncthreads();
+    // K pass
+    int conducting = 0;
+    int c0 = 0;
+    for (int c = 0; c < ncolors; c++) {
+        const int c1 = Bp->col_end[c];
+        for (int i = c0 + tid; i < c1; i += BT) {
+            const int64_t r = (int64_t)rec0 + i;
+            tile_element<true, Q4, kStiffness>(A, r, slot, incv, nnz, ninc);
+            if (!conducting) {
+                const double sg = I.sigma ? __ldg(I.sigma + __ldg(A.recs + 2 * A.nrec + r).z) : 1.0;
+                conducting = fabs(sg) > 1e-12;
+            }
+        }
+        c0 = c1;
+        if (c + 1 == ncolors) cp_async_wait_all();
+        __syncthreads();
+    }
+    if (ncolors == 0) {
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    tile_rows_diag<BT, true>(srows, nrows, incv, ninc, slot, nnz, A.err);
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int c = warp; c < nchunks; c += BT / 32) {
+        const uint2 ch = schunks[c];
+        const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
+        const int64_t g = (int64_t)ch.y;
+        if (sb0 + len > nnz || g + len > A.nnz_total) {
+            if (lane == 0) flag(A.err);
+            continue;
+        }
+        for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i)] = slot[sb0 + i];
+    }
+    // block-uniform: does any element of the block conduct? (also the barrier after the stores)
+    const bool any_m = __syncthreads_or(conducting) != 0;
+    if (any_m) {
+        for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
+        __syncthreads();
+        c0 = 0;
+        for (int c = 0; c < ncolors; c++) {
+            const int c1 = Bp->col_end[c];
+            for (int i = c0 + tid; i < c1; i += BT) tile_mass_element(I, (int64_t)rec0 + i, slot, incv, nnz, ninc, sval);
+            c0 = c1;
+            __syncthreads();
+        }
+        tile_rows_diag<BT, false>(srows, nrows, incv, ninc, slot, nnz, A.err);
+        __syncthreads();
+    }
+    for (int c = warp; c < nchunks; c += BT / 32) {
+        const uint2 ch = schunks[c];
+        const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
+        const int64_t g = (int64_t)ch.y;
+        if (sb0 + len > nnz || g + len > A.nnz_total) continue;  // flagged in the K pass
+        for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i) + 1] = I.omega * (any_m ? slot[sb0 + i] : 0.0);
+    }
+}
+
 // 320 threads: a colour class of an interior 4x4x4 tile holds about 288 elements, so each
 // colour phase runs in one pass (256 threads left a second pass with one warp busy).
 constexpr int kTileBT = 320;
@@ -886,6 +1073,103 @@ int launch_tile_seeded(const TilePlan &tp, const ElemData &m, const double *sol,
     size_t smem = tile_smem_bytes(tp, &a);
     const bool q4 = qp.nq == 4 && qp.uniform_w;
     return q4 ? launch<true, true, kSeeded>(a, tp, smem, s) : launch<true, false, kSeeded>(a, tp, smem, s);
+}
+
+namespace {
+
+using ComplexKernel = void (*)(const TileComplexInstance *, const int2 *, int, int, int, int, int, int);
+
+ComplexKernel complex_kernel(int variant, bool q4) {
+    if (q4) return variant == 1 ? k_tile_complex<288, 2, true> : k_tile_complex<320, 2, true>;
+    return variant == 1 ? k_tile_complex<288, 2, false> : k_tile_complex<320, 2, false>;
+}
+constexpr int kComplexThreads[kTileComplexVariants] = {320, 288};
+
+}  // namespace
+
+int build_tile_complex(const std::vector<TileComplexInput> &in, TileComplexBatch *b, cudaStream_t s) {
+    *b = TileComplexBatch{};
+    if (in.empty()) return MAG_OK;
+    std::vector<TileComplexInstance> hi(in.size());
+    int q4 = 1;
+    for (size_t i = 0; i < in.size(); i++) {
+        const TilePlan &tp = *in[i].tp;
+        if (!tp.ok || !in[i].qp.standard_curl || in[i].qp.nq > kMaxQuad) return MAG_OK;
+        TileComplexInstance &t = hi[i];
+        t = TileComplexInstance{};
+        t.a = make_args(tp, in[i].m, in[i].qp, in[i].err);
+        t.a.nu_e = in[i].nu;
+        t.a.nnz_total = tp.nnz;
+        t.sigma = in[i].sigma;
+        t.val_ref = in[i].qp.val_ref;
+        t.omega = in[i].omega;
+        t.cvals = in[i].vals;
+        b->smem_nnz = std::max(b->smem_nnz, (tp.max_nnz + 1) & ~1);
+        b->smem_inc = std::max(b->smem_inc, tp.max_inc);
+        b->smem_rows = std::max(b->smem_rows, tp.max_rows);
+        b->smem_chunks = std::max(b->smem_chunks, tp.max_chunks);
+        q4 &= (in[i].qp.nq == 4 && in[i].qp.uniform_w) ? 1 : 0;
+    }
+    // items: larger meshes first (a short tail), each mesh's blocks in plan order
+    std::vector<int> order(in.size());
+    for (size_t i = 0; i < in.size(); i++) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return in[x].tp->nrec > in[y].tp->nrec; });
+    std::vector<int2> items;
+    for (int i : order)
+        for (int k = 0; k < in[i].tp->nblocks; k++) items.push_back(make_int2(i, k));
+    if (items.empty() || items.size() >= (size_t)INT32_MAX) return MAG_OK;
+    b->q4 = q4;
+    b->smem = (size_t)b->smem_nnz * sizeof(double) + (size_t)b->smem_inc * sizeof(double2) +
+              (size_t)(b->smem_rows + b->smem_chunks) * sizeof(uint2) + (size_t)18 * kMaxQuad * sizeof(double);
+    int dev = 0, nsm = 0;
+    MAG_CUDA_TRY(cudaGetDevice(&dev));
+    MAG_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    for (int v = 0; v < kTileComplexVariants; v++) {
+        const ComplexKernel kern = complex_kernel(v, q4 != 0);
+        int per = 0;
+        if (cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)kern, kComplexThreads[v], b->smem) !=
+                cudaSuccess || per < 1) {
+            cudaGetLastError();
+            *b = TileComplexBatch{};
+            return MAG_OK;  // the blocks do not fit: the other batch variants remain
+        }
+        b->ahead[v] = per * nsm;
+    }
+    if (cudaMalloc(&b->inst, hi.size() * sizeof(TileComplexInstance)) != cudaSuccess ||
+        cudaMalloc(&b->items, items.size() * sizeof(int2)) != cudaSuccess) {
+        cudaGetLastError();
+        free_tile_complex(b);
+        return MAG_OK;
+    }
+    MAG_CUDA_TRY(cudaMemcpyAsync(b->inst, hi.data(), hi.size() * sizeof(TileComplexInstance), cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaMemcpyAsync(b->items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+    MAG_CUDA_TRY(cudaStreamSynchronize(s));
+    b->nitems = (int)items.size();
+    b->ok = 1;
+    return MAG_OK;
+}
+
+int launch_tile_complex(const TileComplexBatch &b, int variant, cudaStream_t s) {
+    if (!b.ok || variant < 0 || variant >= kTileComplexVariants) return MAG_E_UNSUPPORTED;
+    const ComplexKernel kern = complex_kernel(variant, b.q4 != 0);
+    kern<<<b.nitems, kComplexThreads[variant], b.smem, s>>>(static_cast<const TileComplexInstance *>(b.inst), b.items,
+                                                           b.nitems, b.ahead[variant], b.smem_nnz, b.smem_inc,
+                                                           b.smem_rows, b.smem_chunks);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+const char *tile_complex_variant_name(int v) {
+    static const char *names[kTileComplexVariants] = {"tile blocks, 320 threads x 2 CTAs/SM",
+                                                      "tile blocks, 288 threads x 2 CTAs/SM"};
+    return v >= 0 && v < kTileComplexVariants ? names[v] : "";
+}
+
+void free_tile_complex(TileComplexBatch *b) {
+    if (b->inst) cudaFree(b->inst);
+    if (b->items) cudaFree(b->items);
+    *b = TileComplexBatch{};
 }
 
 }  // namespace mag

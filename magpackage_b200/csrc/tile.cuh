@@ -109,6 +109,39 @@ int launch_tile_seeded(const TilePlan &tp, const ElemData &m, const double *sol,
                        const QuadParams &qp, const MaterialParams &mp, double *vals, double *res, int *err,
                        cudaStream_t s);
 const char *tile_variant_name(int v);
+
+// Batched complex assembly A_i = K_i(nu_i) + j omega_i M_i(sigma_i) over the tile blocks of
+// many meshes: one CTA per (mesh, block) item; K pass then, where the block holds a
+// conducting element, M pass over the same shared-memory slots.
+struct TileComplexInput {
+    const TilePlan *tp;
+    ElemData m;
+    QuadParams qp;
+    const double *nu;     // [Ne]
+    const double *sigma;  // [Ne] or NULL (sigma = 1 everywhere)
+    double omega;
+    double *vals;         // complex128 [nnz] as (re, im) pairs
+    int *err;             // the mesh's status word
+};
+
+constexpr int kTileComplexVariants = 2;
+
+struct TileComplexBatch {
+    void *inst = nullptr;   // device array of the per-mesh launch arguments
+    int2 *items = nullptr;  // device (mesh, block), larger meshes first
+    int nitems = 0, q4 = 0;
+    int smem_nnz = 0, smem_inc = 0, smem_rows = 0, smem_chunks = 0;
+    size_t smem = 0;
+    int ahead[kTileComplexVariants] = {0, 0};  // CTAs resident at once per launch shape
+    int ok = 0;
+};
+
+// Builds the work queue; leaves b->ok = 0 (and returns MAG_OK) when some mesh has no tile
+// plan or a non-standard curl table.
+int build_tile_complex(const std::vector<TileComplexInput> &in, TileComplexBatch *b, cudaStream_t s);
+int launch_tile_complex(const TileComplexBatch &b, int variant, cudaStream_t s);
+const char *tile_complex_variant_name(int v);
+void free_tile_complex(TileComplexBatch *b);
 // K(nu) with per-element reluctivity nu [Ne].
 int launch_tile_stiffness(const TilePlan &tp, const ElemData &m, const double *nu, const QuadParams &qp,
                           double *vals, int *err, cudaStream_t s);
