@@ -312,6 +312,29 @@ __device__ __forceinline__ bool run_layer(Smem &S, const __nv_bfloat16 *W, int K
     return !any_fail;
 }
 
+// The forward kernel's layer: one block-wide barrier per layer. The barrier before the
+// MMA issue also settles whether any thread's previous wait gave up (`ok` is this
+// thread's outcome of its last wait): then every thread leaves the tile loop together.
+// A wait that gives up drains as in run_layer.
+__device__ __forceinline__ bool run_layer_fwd(Smem &S, const __nv_bfloat16 *W, int K, uint32_t &phase,
+                                              long long limit, bool &ok) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // smem writes -> tensor core
+    tc_fence_before();
+    if (__syncthreads_or(ok ? 0 : 1) != 0) {
+        if (threadIdx.x == 0) S.fail = 1;
+        return false;
+    }
+    if (threadIdx.x == 0) {
+        tc_fence_after();
+        mma_issue(S.tmem, S.act, W, K, &S.bar);
+    }
+    ok = mbar_wait(&S.bar, phase, limit);
+    if (!ok) mbar_wait(&S.bar, phase);
+    phase ^= 1u;
+    tc_fence_after();
+    return true;
+}
+
 // ---- forward ---------------------------------------------------------------------
 
 // INFER: no pre-activations kept (prediction); the epilogues use the packed forms above.
@@ -339,6 +362,7 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
     const __nv_bfloat16 *W1 = S.w, *W2 = S.w + kW1pElems, *W3 = S.w + kW1pElems + kWElems;
     const float *sb1 = S.vec, *sb2 = S.vec + kH, *sb3 = S.vec + 2 * kH, *sw4 = S.vec + 3 * kH;
     uint32_t phase = 0;
+    bool ok = true;  // this thread's last tensor-core wait completed
     // The next tile's feature row (one 16-byte load: feature rows are 16 bytes, the buffer
     // 16-byte aligned) and output index are loaded one tile ahead, so their DRAM latency
     // overlaps the current tile's layers.
@@ -380,16 +404,17 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
         float *zr = (a.z_out && valid) ? a.z_out + row * 3 * kH : nullptr;
         // layer 1
         // (a completed MMA has read its input image; the next layer's issue barrier orders
-        // this thread's TMEM reads and image writes before the next MMA)
-        if (!run_layer(S, W1, 16, phase, a.spin_limit)) break;
+        // every thread's TMEM reads and image writes before the next MMA, also across tiles:
+        // the next tile's first MMA is issued after its own barrier)
+        if (!run_layer_fwd(S, W1, 16, phase, a.spin_limit, ok)) break;
         if (INFER) hidden_epilogue_infer(S.tmem, sb1, S.act, t);
         else hidden_epilogue(S.tmem, sb1, S.act, t, zr);
         // layer 2
-        if (!run_layer(S, W2, kH, phase, a.spin_limit)) break;
+        if (!run_layer_fwd(S, W2, kH, phase, a.spin_limit, ok)) break;
         if (INFER) hidden_epilogue_infer(S.tmem, sb2, S.act, t);
         else hidden_epilogue(S.tmem, sb2, S.act, t, zr ? zr + kH : nullptr);
         // layer 3 and the 64 -> 1 output, 16 columns at a time
-        if (!run_layer(S, W3, kH, phase, a.spin_limit)) break;
+        if (!run_layer_fwd(S, W3, kH, phase, a.spin_limit, ok)) break;
         float y = 0.0f;
         if (INFER) {  // pairs: single-precision tanh (the output is not rounded to BF16)
             const uint64_t half2 = pk2(0.5f, 0.5f);
@@ -430,7 +455,7 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
             }
         }
         y += S.vec[4 * kH];
-        if (valid) {
+        if (valid && ok) {  // (after a wait that gave up, the kernel reports a timeout instead)
             if (a.y_out) a.y_out[row] = y;
             if (a.nu_out) {  // nu = exp(y * scale + shift), clamped to [nu_min, nu_max]
                 double v = exp((double)y * a.y_scale + a.y_shift);
@@ -438,11 +463,10 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
                 a.nu_out[dst] = v;
             }
         }
-        tc_fence_before();
-        __syncthreads();
     }
+    if (!ok) S.fail = 1;  // a wait of the last layer gave up
+    tmem_free(S);         // (its barrier makes S.fail visible to thread 0)
     if (t == 0 && S.fail && a.err) atomicExch(a.err, 1);
-    tmem_free(S);
 }
 
 // ---- backward --------------------------------------------------------------------

@@ -17,11 +17,10 @@
 //              colour share an entry (the face-adjacency graph of a Kuhn mesh is
 //              bipartite: two colours), and the colours run one after another.
 //              Diagonal entries and residual entries go to per-incidence slots.
-//   chunk phase -- the block's rows form runs of consecutive rows, contiguous in the
-//              CSR, cut at row boundaries into store chunks of at most 256 nonzeros.
-//              Per chunk one warp sums the diagonal and residual contributions of the
-//              chunk's rows in ascending element order (the reference's sparse() order),
-//              one lane per row, then stores the chunk's nonzeros, coalesced.
+//   row phase -- one thread per row sums its diagonal and residual contributions in
+//              ascending element order (the reference's sparse() order).
+//   store phase -- the block's rows form runs of consecutive rows, contiguous in the
+//              CSR; warps store them in chunks, coalesced.
 // No floating-point atomics; results equal the reference's MEX + sparse() bit for bit.
 #include <omp.h>
 
@@ -219,56 +218,6 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Row r of the block: its incidence slots summed in ascending element order. The
-// residual (component x, when !STIFF) goes to res[row]; the diagonal (component DIAG_Y ?
-// y : x, when CALCJ) to the row's diagonal nonzero.
-template <bool CALCJ, bool STIFF, int DIAG_Y>
-__device__ __forceinline__ void tile_row_sums(const TileArgs &A, const uint2 *srows, int r, int nrows,
-                                              const double2 *incv, int ninc, double *slot, int nnz) {
-    const uint2 rw = srows[r];
-    const int nzb = (int)(rw.y & 0x1FFFu), incb = (int)((rw.y >> 13) & 0xFFFu);
-    const int diag = (int)((rw.y >> 25) & 31u);
-    int ince = r + 1 < nrows ? (int)((srows[r + 1].y >> 13) & 0xFFFu) : ninc;
-    if (ince > ninc) ince = ninc;
-    double racc = 0.0, dacc = 0.0;
-    for (int k = incb; k < ince; k++) {
-        const double2 v = incv[k];
-        if (!STIFF) racc = racc + v.x;
-        if (CALCJ) dacc = dacc + (DIAG_Y ? v.y : v.x);
-    }
-    if (!STIFF) {
-        if ((int64_t)rw.x < A.ndof) A.res[rw.x] = racc;
-        else flag(A.err);
-    }
-    if (CALCJ && ince > incb) {
-        if (nzb + diag < nnz) slot[nzb + diag] = dacc;
-        else flag(A.err);
-    }
-}
-
-// Store chunk c of a block: block nonzeros [sb0, sb1) go to global nonzeros [g, g + sb1 - sb0);
-// it owns block rows [r0, r1). Chunks tile the block's nonzeros and rows in order.
-struct TileChunk {
-    int sb0, sb1, r0, r1;
-    int64_t g;
-};
-__device__ __forceinline__ TileChunk chunk_at(const uint2 *schunks, int c, int nchunks, int nnz, int nrows) {
-    const uint2 ch = schunks[c];
-    TileChunk t;
-    t.sb0 = (int)(ch.x & 0xFFFFu);
-    t.r0 = (int)(ch.x >> 16);
-    t.g = (int64_t)ch.y;
-    t.sb1 = nnz;
-    t.r1 = nrows;
-    if (c + 1 < nchunks) {
-        const uint32_t x1 = schunks[c + 1].x;
-        t.sb1 = (int)(x1 & 0xFFFFu);
-        t.r1 = (int)(x1 >> 16);
-    }
-    if (t.r1 > nrows) t.r1 = nrows;
-    return t;
-}
-
 // One CTA per block. The CTA of block b prefetches into L2 the records of block b + ahead
 // (ahead = the CTAs resident at once), the block the hardware starts about when b ends.
 // The block's row table and store chunks are copied into shared memory while its
@@ -319,24 +268,41 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int 
             cp_async_wait_all();
             __syncthreads();
         }
+        // rows: diagonal and residual in ascending element order
+        for (int r = tid; r < nrows; r += BT) {
+            const uint2 rw = srows[r];
+            const int nzb = (int)(rw.y & 0x1FFFu), incb = (int)((rw.y >> 13) & 0xFFFu);
+            const int diag = (int)((rw.y >> 25) & 31u);
+            int ince = r + 1 < nrows ? (int)((srows[r + 1].y >> 13) & 0xFFFu) : ninc;
+            if (ince > ninc) ince = ninc;
+            double racc = 0.0, dacc = 0.0;
+            for (int k = incb; k < ince; k++) {
+                const double2 v = incv[k];
+                racc = racc + v.x;
+                if (CALCJ) dacc = dacc + v.y;
+            }
+            if (!STIFF) {
+                if ((int64_t)rw.x < A.ndof) A.res[rw.x] = racc;
+                else flag(A.err);
+            }
+            if (CALCJ && ince > incb) {
+                if (nzb + diag < nnz) slot[nzb + diag] = dacc;
+                else flag(A.err);
+            }
+        }
+        __syncthreads();
         if (CALCJ) {
-            // Per store chunk: the warp sums the diagonals (and residuals) of the rows the
-            // chunk owns, then stores the chunk's nonzeros. A chunk's rows' diagonals lie in
-            // its own nonzeros, so a warp barrier orders the two; no block-wide barrier.
             const int warp = tid >> 5, lane = tid & 31;
             for (int c = warp; c < nchunks; c += BT / 32) {
-                const TileChunk ch = chunk_at(schunks, c, nchunks, nnz, nrows);
-                for (int r = ch.r0 + lane; r < ch.r1; r += 32)
-                    tile_row_sums<CALCJ, STIFF, 1>(A, srows, r, nrows, incv, ninc, slot, nnz);
-                __syncwarp();
-                if (ch.sb0 > ch.sb1 || ch.sb1 > nnz || ch.g + (ch.sb1 - ch.sb0) > A.nnz_total) {
+                const uint2 ch = schunks[c];
+                const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
+                const int64_t g = (int64_t)ch.y;
+                if (sb0 + len > nnz || g + len > A.nnz_total) {
                     if (lane == 0) flag(A.err);
                     continue;
                 }
-                for (int i = lane; i < ch.sb1 - ch.sb0; i += 32) A.vals[ch.g + i] = slot[ch.sb0 + i];
+                for (int i = lane; i < len; i += 32) A.vals[g + i] = slot[sb0 + i];
             }
-        } else {
-            for (int r = tid; r < nrows; r += BT) tile_row_sums<CALCJ, STIFF, 1>(A, srows, r, nrows, incv, ninc, slot, nnz);
         }
     }
 }
@@ -411,6 +377,26 @@ __device__ __forceinline__ void tile_mass_element(const TileComplexInstance &I, 
     }
 }
 
+// Sums each row's diagonal contributions (incidence slots, component x or y) in ascending
+// element order into the row's diagonal nonzero.
+template <int BT, bool COMP_Y>
+__device__ __forceinline__ void tile_rows_diag(const uint2 *srows, int nrows, const double2 *incv, int ninc,
+                                               double *slot, int nnz, int *err) {
+    for (int r = threadIdx.x; r < nrows; r += BT) {
+        const uint2 rw = srows[r];
+        const int nzb = (int)(rw.y & 0x1FFFu), incb = (int)((rw.y >> 13) & 0xFFFu);
+        const int diag = (int)((rw.y >> 25) & 31u);
+        int ince = r + 1 < nrows ? (int)((srows[r + 1].y >> 13) & 0xFFFu) : ninc;
+        if (ince > ninc) ince = ninc;
+        double dacc = 0.0;
+        for (int k = incb; k < ince; k++) dacc = dacc + (COMP_Y ? incv[k].y : incv[k].x);
+        if (ince > incb) {
+            if (nzb + diag < nnz) slot[nzb + diag] = dacc;
+            else flag(err);
+        }
+    }
+}
+
 // One CTA per (mesh, block) item. K pass: the tile kernel's K(nu) elements (incidence
 // slots get (0, K diagonal)), row sums, real parts stored. M pass, only when some element
 // of the block conducts: slots zeroed again, the conducting elements' M rows, row sums,
@@ -471,17 +457,18 @@ __global__ void __launch_bounds__(BT, MINB)
         cp_async_wait_all();
         __syncthreads();
     }
-    // real parts: per chunk, its rows' K diagonals (component y), then its nonzeros
+    tile_rows_diag<BT, true>(srows, nrows, incv, ninc, slot, nnz, A.err);
+    __syncthreads();
     const int warp = tid >> 5, lane = tid & 31;
     for (int c = warp; c < nchunks; c += BT / 32) {
-        const TileChunk ch = chunk_at(schunks, c, nchunks, nnz, nrows);
-        for (int r = ch.r0 + lane; r < ch.r1; r += 32) tile_row_sums<true, true, 1>(A, srows, r, nrows, incv, ninc, slot, nnz);
-        __syncwarp();
-        if (ch.sb0 > ch.sb1 || ch.sb1 > nnz || ch.g + (ch.sb1 - ch.sb0) > A.nnz_total) {
+        const uint2 ch = schunks[c];
+        const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
+        const int64_t g = (int64_t)ch.y;
+        if (sb0 + len > nnz || g + len > A.nnz_total) {
             if (lane == 0) flag(A.err);
             continue;
         }
-        for (int i = lane; i < ch.sb1 - ch.sb0; i += 32) I.cvals[2 * (ch.g + i)] = slot[ch.sb0 + i];
+        for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i)] = slot[sb0 + i];
     }
     // block-uniform: does any element of the block conduct? (also the barrier after the stores)
     const bool any_m = __syncthreads_or(conducting) != 0;
@@ -495,17 +482,15 @@ __global__ void __launch_bounds__(BT, MINB)
             c0 = c1;
             __syncthreads();
         }
+        tile_rows_diag<BT, false>(srows, nrows, incv, ninc, slot, nnz, A.err);
+        __syncthreads();
     }
-    // imaginary parts: omega * M (M diagonals from component x), or omega * 0
     for (int c = warp; c < nchunks; c += BT / 32) {
-        const TileChunk ch = chunk_at(schunks, c, nchunks, nnz, nrows);
-        if (any_m)
-            for (int r = ch.r0 + lane; r < ch.r1; r += 32)
-                tile_row_sums<true, true, 0>(A, srows, r, nrows, incv, ninc, slot, nnz);
-        __syncwarp();
-        if (ch.sb0 > ch.sb1 || ch.sb1 > nnz || ch.g + (ch.sb1 - ch.sb0) > A.nnz_total) continue;  // flagged above
-        for (int i = lane; i < ch.sb1 - ch.sb0; i += 32)
-            I.cvals[2 * (ch.g + i) + 1] = I.omega * (any_m ? slot[ch.sb0 + i] : 0.0);
+        const uint2 ch = schunks[c];
+        const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
+        const int64_t g = (int64_t)ch.y;
+        if (sb0 + len > nnz || g + len > A.nnz_total) continue;  // flagged in the K pass
+        for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i) + 1] = I.omega * (any_m ? slot[sb0 + i] : 0.0);
     }
 }
 
@@ -702,9 +687,7 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
             }
             B.nnz = bn;
             B.ninc = bi;
-            // store chunks: runs of consecutive rows (contiguous in the CSR), cut at row
-            // boundaries into pieces of at most kTileChunk nonzeros; a chunk owns its rows
-            // (x = first block nonzero | first block row << 16, y = first global nonzero)
+            // store chunks: runs of consecutive rows, cut at kTileChunk nonzeros
             std::vector<uint2> &ch = bchunk[b];
             ch.clear();
             {
@@ -713,20 +696,16 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
                 while (k < k1) {
                     int64_t k2 = k + 1;
                     while (k2 < k1 && order[k2] == order[k2 - 1] + 1) k2++;
-                    int64_t a = k;
-                    while (a < k2) {
-                        const int64_t g = row_ptr[order[a]];
-                        int64_t e = a + 1;
-                        while (e < k2 && row_ptr[order[e] + 1] - g <= kTileChunk) e++;
-                        ch.push_back(make_uint2((uint32_t)off | ((uint32_t)(a - k0) << 16), (uint32_t)g));
-                        off += (int32_t)(row_ptr[order[e - 1] + 1] - g);
-                        a = e;
+                    const int64_t g0 = row_ptr[order[k]], g1 = row_ptr[order[k2 - 1] + 1];
+                    for (int64_t g = g0; g < g1; g += kTileChunk) {
+                        const int32_t len = (int32_t)std::min<int64_t>(kTileChunk, g1 - g);
+                        ch.push_back(make_uint2((uint32_t)(off + (g - g0)) | ((uint32_t)len << 16), (uint32_t)g));
                     }
+                    off += (int32_t)(g1 - g0);
                     k = k2;
                 }
             }
             B.nchunks = (int32_t)ch.size();
-            if (B.nrows > 0xFFFF) fail = 1;
             // distinct elements (ascending) and their records
             std::sort(incs.begin(), incs.end(), [](const Inc &x, const Inc &y) {
                 return x.e != y.e ? x.e < y.e : x.l < y.l;
