@@ -271,7 +271,7 @@ def run_transient(args):
     torch.cuda.set_device(0)
     cfg = TransientConfig()
     t0 = time.perf_counter()
-    out = compare(cfg)
+    out = compare(cfg, epochs=args.epochs)
     wall = time.perf_counter() - t0
     p, l, i = out["plain"], out["learned"], out["ideal"]
     steps = l["steps"]
@@ -542,6 +542,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--instances", type=int, default=64, help="meshes of the batched_complex workload")
     ap.add_argument("--tile-variant", type=int, default=None, help="launch shape of the tile Jacobian kernel")
+    ap.add_argument("--epochs", type=int, default=120, help="training epochs of the transient workload's MLP")
     ap.add_argument("--schedule", default="tile-blocks",
                     choices=["tile-blocks", "shared-row-blocks", "nz-row-blocks", "row-blocks", "two-pass"],
                     help="Jacobian assembly schedule (all give identical bits)")
@@ -625,6 +626,11 @@ def main():
         if with_mlp:
             infer()
 
+    tuning = None
+    if sched_id == _lib.SCHEDULE_TILE_BLOCKS and args.tile_variant is None:
+        # the autotuner picks the launch shape and L2 staging depth on this state (untimed)
+        tv, td, tt = plan.tune(sol, vals, res, reps=3)
+        tuning = {"variant": tv, "prefetch_waves": td, "times_ms": np.round(tt, 4).tolist()}
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -752,6 +758,7 @@ def main():
                        "tile_blocks": plan.info.tile_blocks,
                        "element_evaluations_per_element": round(plan.info.tile_evals_per_elem, 4),
                        "plan_build_ms": round(plan.info.tile_plan_ms, 1),
+                       "tile_tuning": tuning,
                        "schedule": {_lib.SCHEDULE_TILE_BLOCKS: "spatial tiles of 4x4x4 node layers: one CTA per "
                                                                "block of whole rows, one thread per incident "
                                                                "element, off-diagonal entries placed in colour "

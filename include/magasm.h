@@ -66,6 +66,9 @@ typedef struct {
 #define MAG_OPTION_SCHEDULE 1
 #define MAG_OPTION_TILE_VARIANT 2 /* launch shape of the tile schedule's Jacobian kernel: 0 = 320 threads x
                                      2 CTAs/SM (default), 1 = 288 x 2, 2 = 256 x 2, 3 = 512 x 1; same bits */
+#define MAG_OPTION_TILE_PREFETCH 3 /* staging depth of the tile schedule: how many waves of resident CTAs
+                                      ahead a CTA prefetches its successor block's records into L2
+                                      (0 = none, 1 = default, 2); same bits */
 #define MAG_SCHEDULE_TWO_PASS 0   /* element kernel + row reduction through an HBM scratch slab */
 #define MAG_SCHEDULE_RETIRED_1 1  /* retired (a persistent launch over an L2 scratch ring); rejected */
 #define MAG_SCHEDULE_ROW_BLOCKS 2 /* one launch, no scratch: per-row element recompute */
@@ -119,6 +122,14 @@ int mag_mesh_destroy(mag_mesh *mesh);
 int mag_mesh_get_info(const mag_mesh *mesh, mag_mesh_info *info);
 /* Handle options (MAG_OPTION_*). */
 int mag_mesh_set_option(mag_mesh *mesh, int option, int64_t value);
+/* Autotune the tile schedule's Newton Jacobian on the caller's state: every launch shape
+ * (MAG_OPTION_TILE_VARIANT) x staging depth (MAG_OPTION_TILE_PREFETCH) is timed `reps` times
+ * (CUDA events on `stream`) and the fastest is kept in the handle. times_ms, when not NULL,
+ * receives the mean ms of each pair, index variant * 3 + depth (12 entries). The outputs of
+ * every candidate are the same bits, so d_vals and d_res hold the Jacobian and residual at
+ * d_sol afterwards. MAG_E_UNSUPPORTED when the mesh runs another schedule. */
+int mag_mesh_tune(mag_mesh *mesh, const double *d_sol, double *d_vals, double *d_res, int reps,
+                  double *times_ms, int *variant, int *depth, void *stream);
 /* Synchronise `stream` and report whether the last assemblies completed: MAG_E_RANGE if a
  * kernel of the tile schedule found a plan index out of range and skipped it (an internal
  * error: the results are incomplete). The status is cleared once reported. No assembly

@@ -48,6 +48,7 @@ _PROTOS = {
     "mag_mesh_get_info": ([_vp, C.POINTER(MeshInfo)], _int),
     "mag_mesh_pattern": ([_vp, _vp, _vp, _vp], _int),
     "mag_mesh_set_option": ([_vp, _int, _i64], _int),
+    "mag_mesh_tune": ([_vp, _vp, _vp, _vp, _int, _vp, C.POINTER(_int), C.POINTER(_int), _vp], _int),
     "mag_mesh_check": ([_vp, _vp], _int),
     "mag_mesh_set_quadrature": ([_vp, _dp, _int, _dp, _dp], _int),
     "mag_mesh_set_materials": ([_vp, _dp, _dp, _dp, _int, _dp, _int, _dp, _int, _dp, _dp, _dp], _int),

@@ -779,8 +779,68 @@ int mag_mesh_set_option(mag_mesh *m, int option, int64_t value) {
         m->tile.variant = (int)value;
         return MAG_OK;
     }
+    if (option == MAG_OPTION_TILE_PREFETCH) {
+        if (value < 0 || value >= kTileDepths) {
+            set_error("tile prefetch depth %lld out of range (0..%d)", (long long)value, kTileDepths - 1);
+            return MAG_E_ARG;
+        }
+        m->tile.prefetch_waves = (int)value;
+        return MAG_OK;
+    }
     set_error("unknown option %d", option);
     return MAG_E_ARG;
+}
+
+int mag_mesh_tune(mag_mesh *m, const double *d_sol, double *d_vals, double *d_res, int reps, double *times_ms,
+                  int *variant, int *depth, void *stream) {
+    if (!m || !d_sol || !d_vals || !d_res || reps < 1) {
+        set_error("mag_mesh_tune: bad arguments");
+        return MAG_E_ARG;
+    }
+    if (m->schedule != MAG_SCHEDULE_TILE_BLOCKS || !m->tile.ok) {
+        set_error("mag_mesh_tune: the mesh does not run the tile schedule");
+        return MAG_E_UNSUPPORTED;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    MAG_CUDA_TRY(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return MAG_E_CUDA;
+    }
+    const int v0 = m->tile.variant, w0 = m->tile.prefetch_waves;
+    int best_v = v0, best_w = w0, rc = MAG_OK;
+    double best = 1e300;
+    for (int v = 0; v < kTileVariants && rc == MAG_OK; v++)
+        for (int w = 0; w < kTileDepths && rc == MAG_OK; w++) {
+            m->tile.variant = v;
+            m->tile.prefetch_waves = w;
+            rc = mag_assemble_jacobian(m, d_sol, d_vals, d_res, 1, stream);  // warm-up
+            if (rc != MAG_OK) break;
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < reps && rc == MAG_OK; r++) rc = mag_assemble_jacobian(m, d_sol, d_vals, d_res, 1, stream);
+            cudaEventRecord(e1, s);
+            if (cudaEventSynchronize(e1) != cudaSuccess) rc = MAG_E_CUDA;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const double t = (double)ms / reps;
+            if (times_ms) times_ms[v * kTileDepths + w] = t;
+            if (rc == MAG_OK && t < best) {
+                best = t;
+                best_v = v;
+                best_w = w;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    m->tile.variant = rc == MAG_OK ? best_v : v0;
+    m->tile.prefetch_waves = rc == MAG_OK ? best_w : w0;
+    if (rc != MAG_OK) return rc;
+    // the kept pair's outputs (every candidate gives the same bits)
+    MAG_TRY(mag_assemble_jacobian(m, d_sol, d_vals, d_res, 1, stream));
+    if (variant) *variant = best_v;
+    if (depth) *depth = best_w;
+    return MAG_OK;
 }
 
 int mag_mesh_check(mag_mesh *m, void *stream) {

@@ -236,9 +236,10 @@ __device__ __forceinline__ void hidden_epilogue_infer(uint32_t tmem, const float
         tmem_cols16(tmem, c, z);
         __align__(16) uint32_t hp[8];
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const float2 b = *reinterpret_cast<const float2 *>(bias + c + 2 * i);
+        for (int i = 0; i < 8; i += 2) {  // one 16-byte shared load of biases per two pairs
+            const float4 b = *reinterpret_cast<const float4 *>(bias + c + 2 * i);
             hp[i] = silu2_bf16(add2(pk2(z[2 * i], z[2 * i + 1]), pk2(b.x, b.y)));
+            hp[i + 1] = silu2_bf16(add2(pk2(z[2 * i + 2], z[2 * i + 3]), pk2(b.z, b.w)));
         }
         *reinterpret_cast<uint4 *>(img + core_off(row_t, c, kH)) = *reinterpret_cast<uint4 *>(hp);
         *reinterpret_cast<uint4 *>(img + core_off(row_t, c + 8, kH)) = *reinterpret_cast<uint4 *>(hp + 4);
@@ -425,8 +426,14 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
                 tmem_cols16(S.tmem, c, z);
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
-                    const float2 b = *reinterpret_cast<const float2 *>(sb3 + c + 2 * i);
-                    const float2 w = *reinterpret_cast<const float2 *>(sw4 + c + 2 * i);
+                    // biases and output weights by 16-byte shared loads, two pairs each
+                    float4 b4, w4;
+                    if ((i & 1) == 0) {
+                        b4 = *reinterpret_cast<const float4 *>(sb3 + c + 2 * i);
+                        w4 = *reinterpret_cast<const float4 *>(sw4 + c + 2 * i);
+                    }
+                    const float2 b = (i & 1) ? make_float2(b4.z, b4.w) : make_float2(b4.x, b4.y);
+                    const float2 w = (i & 1) ? make_float2(w4.z, w4.w) : make_float2(w4.x, w4.y);
                     const uint64_t zz = add2(pk2(z[2 * i], z[2 * i + 1]), pk2(b.x, b.y));
                     float h0, h1, t0, t1;
                     upk2(mul2(zz, half2), h0, h1);

@@ -997,7 +997,9 @@ int launch(const TileArgs &a, const TilePlan &tp, size_t smem, cudaStream_t s) {
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, BT, smem) != cudaSuccess || per < 1)
         return MAG_E_CUDA;
-    kern<<<tp.nblocks, BT, smem, s>>>(a, tp.nblocks, per * nsm);
+    // (ahead >= nblocks: no CTA prefetches)
+    const int ahead = tp.prefetch_waves > 0 ? per * nsm * tp.prefetch_waves : tp.nblocks;
+    kern<<<tp.nblocks, BT, smem, s>>>(a, tp.nblocks, ahead);
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
 

@@ -15,6 +15,7 @@ constexpr int kTileMaxInc = 4095;   // (row, element) incidences per block (12-b
 constexpr int kTileMaxColors = 8;   // element colour classes per block
 constexpr int kTileChunk = 256;     // nonzeros per store chunk (one warp stores a chunk)
 constexpr int kTileVariants = 4;    // launch shapes of the Jacobian kernel (tile_variant_name)
+constexpr int kTileDepths = 3;      // L2 staging depths, in waves of resident CTAs (0, 1, 2)
 constexpr uint32_t kTileAbsent = 0xFFFFFFFFu;
 
 // One CTA's work: whole CSR rows whose edges start in one spatial tile of nodes, and
@@ -56,6 +57,7 @@ struct TilePlan {
     int64_t bytes = 0;
     int ok = 0;
     int variant = 0;  // launch shape of the Newton Jacobian (0 .. kTileVariants-1)
+    int prefetch_waves = 1;  // staging depth: a CTA prefetches the block this many waves ahead (0: none)
 };
 
 struct TilePlanInput {

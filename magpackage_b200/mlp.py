@@ -132,21 +132,25 @@ class NuPredictor:
         xn = self._norm(feats)
         tn = ((ly - self.y_mean) / self.y_std).float().contiguous()
         n = xn.shape[0]
-        g = torch.Generator(device="cpu").manual_seed(seed)
+        # permutations drawn on the device and the loss summed there: no host round trip
+        # per minibatch, so the steps run back to back on the GPU
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
         hist = []
         ybuf = torch.empty(batch, dtype=torch.float32, device="cuda")
         zbuf = torch.empty((batch, 3, 64), dtype=torch.float32, device="cuda")
+        steps = max(1, n // batch)
         for ep in range(epochs):
-            perm = torch.randperm(n, generator=g).to("cuda")
-            tot = 0.0
+            perm = torch.randperm(n, generator=g, device="cuda")
+            tot = torch.zeros((), dtype=torch.float32, device="cuda")
             for i in range(0, n - batch + 1, batch):
                 idx = perm[i:i + batch]
                 xb, tb = xn[idx].contiguous(), tn[idx].contiguous()
                 y = self.mlp.train_step(xb, tb, lr, ybuf, zbuf)
-                tot += float(((y - tb) ** 2).mean())
-            hist.append(tot / max(1, n // batch))
+                tot += ((y - tb) ** 2).mean()
+            hist.append(tot)
         self.mlp.check()
-        return hist
+        return [float(h) / steps for h in hist]
 
     def predict_nu(self, feats: torch.Tensor, rows: torch.Tensor, nu_out: torch.Tensor, nu_min: float,
                    nu_max: float):

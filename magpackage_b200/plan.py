@@ -82,6 +82,21 @@ class AssemblyPlan:
         """Launch shape of the tile schedule's Jacobian kernel (MAG_OPTION_TILE_VARIANT)."""
         _lib.check(self._lib.mag_mesh_set_option(self._h, 2, int(variant)))
 
+    def set_tile_prefetch(self, waves: int):
+        """Staging depth of the tile schedule in waves of resident CTAs (MAG_OPTION_TILE_PREFETCH)."""
+        _lib.check(self._lib.mag_mesh_set_option(self._h, 3, int(waves)))
+
+    def tune(self, sol, vals, res, reps: int = 3, stream=None):
+        """Time every launch shape x staging depth of the tile Jacobian on this state and keep the
+        fastest (mag_mesh_tune); returns (variant, depth, times_ms[4][3]). vals and res hold the
+        Jacobian and residual at sol afterwards."""
+        times = np.zeros(12)
+        v, d = C.c_int(), C.c_int()
+        _lib.check(self._lib.mag_mesh_tune(self._h, _ptr(sol), _ptr(vals), _ptr(res), int(reps),
+                                           times.ctypes.data_as(C.c_void_p), C.byref(v), C.byref(d),
+                                           _lib.stream_ptr(stream)))
+        return v.value, d.value, times.reshape(4, 3)
+
     def check(self, stream=None):
         """Synchronise and raise if a bounded device-side wait gave up."""
         _lib.check(self._lib.mag_mesh_check(self._h, _lib.stream_ptr(stream)))

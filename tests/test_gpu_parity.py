@@ -649,6 +649,22 @@ def test_tile_schedule_shuffled_numbering_and_unused_dofs(oracle_port):
         assert torch.equal(r.view(torch.int64), r3.view(torch.int64)), variant
     with pytest.raises(_lib.MagError):
         plan.set_tile_variant(4)
+    for waves in (0, 2, 1):  # every staging depth too
+        plan.set_tile_prefetch(waves)
+        v3, r3 = plan.jacobian(x)
+        plan.check()
+        assert torch.equal(v.view(torch.int64), v3.view(torch.int64)), waves
+    with pytest.raises(_lib.MagError):
+        plan.set_tile_prefetch(3)
+    # the autotuner times all 12 pairs, keeps one, and leaves the same bits in its outputs
+    vt, rt = plan.new_values(), plan.new_vector()
+    variant, depth, times = plan.tune(x, vt, rt, reps=2)
+    plan.check()
+    assert 0 <= variant < 4 and 0 <= depth < 3 and np.all(times > 0) and times[variant, depth] == times.min()
+    assert torch.equal(v.view(torch.int64), vt.view(torch.int64)) and torch.equal(r.view(torch.int64),
+                                                                                    rt.view(torch.int64))
+    v4, _ = plan.jacobian(x)
+    assert torch.equal(v.view(torch.int64), v4.view(torch.int64))
     nu = np.random.default_rng(5).uniform(0.2, 5.0, T.shape[0]) * material.NU0
     Ik, Jk, Vk = oracle_port.curl_curl(m, nu, qw, curl)
     assert_csr_equal(plan.row_ptr, plan.col_idx, plan.stiffness(dev(nu)), oracle_matrix(oracle_port, Ik, Jk, Vk, n, False))
