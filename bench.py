@@ -271,7 +271,7 @@ def run_transient(args):
     torch.cuda.set_device(0)
     cfg = TransientConfig()
     t0 = time.perf_counter()
-    out = compare(cfg, epochs=args.epochs)
+    out = compare(cfg, epochs=args.epochs, batch=args.train_batch, lr=args.lr)
     wall = time.perf_counter() - t0
     p, l, i = out["plain"], out["learned"], out["ideal"]
     steps = l["steps"]
@@ -542,7 +542,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--instances", type=int, default=64, help="meshes of the batched_complex workload")
     ap.add_argument("--tile-variant", type=int, default=None, help="launch shape of the tile Jacobian kernel")
-    ap.add_argument("--epochs", type=int, default=120, help="training epochs of the transient workload's MLP")
+    ap.add_argument("--epochs", type=int, default=10, help="training epochs of the transient workload's MLP")
+    ap.add_argument("--train-batch", type=int, default=8192, help="minibatch of that training")
+    ap.add_argument("--lr", type=float, default=2e-3, help="Adam step size of that training")
     ap.add_argument("--schedule", default="tile-blocks",
                     choices=["tile-blocks", "shared-row-blocks", "nz-row-blocks", "row-blocks", "two-pass"],
                     help="Jacobian assembly schedule (all give identical bits)")

@@ -2,6 +2,8 @@
 // MEX-compatible entry points.
 #include <omp.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstring>
 #include <memory>
@@ -222,21 +224,50 @@ int upload_materials(const double *lin, const double *isnon, const double *maxb,
             return MAG_E_RANGE;
         }
     }
-    size_t nd = (size_t)3 * nmat + nbrk + ncoe, ni = (size_t)3 * nmat;
+    // doubles: lin | isnon | maxb | breaks | coefs | bucket geometry (2 per material);
+    // ints: start | count | coef_start | bucket windows (2 kMatBuckets per material)
+    size_t nd = (size_t)5 * nmat + nbrk + ncoe, ni = (size_t)3 * nmat + (size_t)2 * kMatBuckets * nmat;
     size_t bytes = nd * 8 + ni * 4 + 64;
     char *host = new (std::nothrow) char[bytes];
     if (!host) return MAG_E_NOMEM;
+    std::memset(host, 0, bytes);
     double *hd = reinterpret_cast<double *>(host);
     std::memcpy(hd, lin, nmat * 8);
     std::memcpy(hd + nmat, isnon, nmat * 8);
     std::memcpy(hd + 2 * nmat, maxb, nmat * 8);
     if (nbrk) std::memcpy(hd + 3 * nmat, brk, nbrk * 8);
     if (ncoe) std::memcpy(hd + 3 * nmat + nbrk, coe, ncoe * 8);
+    double *geom = hd + 3 * nmat + nbrk + ncoe;
     int *hi = reinterpret_cast<int *>(hd + nd);
     for (int m = 0; m < nmat; m++) {
         hi[m] = (int)start[m];
         hi[nmat + m] = (int)cnt[m];
         hi[2 * nmat + m] = (int)coestart[m];
+    }
+    // Search windows of the spline lookup (see material_eval): for a table of strictly
+    // increasing finite breaks below a finite MaxBSq, kMatBuckets buckets uniform in s from
+    // the first break to MaxBSq; bucket i's window is [K(e(i-1)), K(e(i+2))] with K(y) the
+    // last break <= y (0 if none) and e(j) = origin + j / scale. Other tables keep scale 0.
+    int *win = hi + 3 * nmat;
+    for (int m = 0; m < nmat; m++) {
+        if (isnon[m] == 0.0) continue;
+        const int st = (int)start[m], c = (int)cnt[m];
+        const double *b = brk + st, smax = maxb[m];
+        bool ok = std::isfinite(smax) && std::isfinite(b[0]) && smax > b[0];
+        for (int j = 1; j < c && ok; j++) ok = std::isfinite(b[j]) && b[j] > b[j - 1];
+        const double scale = ok ? (double)kMatBuckets / (smax - b[0]) : 0.0;
+        if (!(scale > 0.0) || !std::isfinite(scale)) continue;
+        auto K = [&](double y) {
+            const int j = (int)(std::upper_bound(b, b + c, y) - b) - 1;
+            return j < 0 ? 0 : j;
+        };
+        int *lo = win + 2 * kMatBuckets * m, *up = lo + kMatBuckets;
+        for (int i = 0; i < kMatBuckets; i++) {
+            lo[i] = K(b[0] + (double)(i - 1) / scale);
+            up[i] = K(b[0] + (double)(i + 2) / scale);
+        }
+        geom[2 * m] = b[0];
+        geom[2 * m + 1] = scale;
     }
     void *dmem = nullptr;
     cudaError_t ce = cudaMalloc(&dmem, bytes);
@@ -258,7 +289,8 @@ int upload_materials(const double *lin, const double *isnon, const double *maxb,
     double *dd = static_cast<double *>(dmem);
     int *di = reinterpret_cast<int *>(dd + nd);
     out->mp = MaterialParams{nmat, nbrk, ncoe, dd, dd + nmat, dd + 2 * nmat, dd + 3 * nmat,
-                             dd + 3 * nmat + nbrk, di, di + nmat, di + 2 * nmat};
+                             dd + 3 * nmat + nbrk, di, di + nmat, di + 2 * nmat, di + 3 * nmat,
+                             dd + 3 * nmat + nbrk + ncoe};
     return MAG_OK;
 }
 

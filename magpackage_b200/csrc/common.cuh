@@ -63,7 +63,16 @@ struct MaterialParams {
     const int *start;
     const int *count;
     const int *coef_start;
+    // Optional windows of the spline search (NULL: binary search over the whole table): per
+    // material kMatBuckets buckets uniform in s = |B|^2 from origin = the first break to
+    // MaxBSq; bucket[2 kMatBuckets m + i] and bucket[2 kMatBuckets m + kMatBuckets + i] are the
+    // window of bucket i; bucket_geom[2m], [2m + 1] = origin, scale (buckets per unit of s;
+    // 0 = this material has no buckets).
+    const int *bucket;
+    const double *bucket_geom;
 };
+
+constexpr int kMatBuckets = 256;
 
 // Element-side mesh data in the handle's layout.
 struct ElemData {

@@ -97,6 +97,21 @@ __device__ __forceinline__ void material_eval(const MaterialParams &mp, int tag,
     const double *b = mp.breaks + __ldg(mp.start + m);
     int pieces = __ldg(mp.count + m);
     int k = 0, lo = 0, hi = pieces - 1;
+    // The last break <= x (0 if none), as the reference's binary search over the whole table
+    // finds it (MexMaterialUtils.hpp:47-59). With buckets, the search runs inside the window
+    // of x's uniform-in-s bucket i: the host stored the answers at the edges e(i-1) and e(i+2),
+    // one bucket wider on each side than the bucket, so the answer for x lies in [lo, hi]
+    // whichever neighbouring bucket the rounding of (x - origin) * scale picks, and the binary
+    // search inside the window returns the same index (NaN or x below the first break: 0).
+    const double scale = mp.bucket ? __ldg(mp.bucket_geom + 2 * m + 1) : 0.0;
+    if (scale > 0.0) {
+        const double f = (x - __ldg(mp.bucket_geom + 2 * m)) * scale;
+        const int i = !(f >= 0.0) ? 0 : (f >= (double)(kMatBuckets - 1) ? kMatBuckets - 1 : (int)f);
+        const int *w = mp.bucket + 2 * kMatBuckets * m + i;
+        lo = __ldg(w);
+        hi = __ldg(w + kMatBuckets);
+        k = lo;
+    }
     while (lo <= hi) {
         int mid = lo + (hi - lo) / 2;
         if (x >= __ldg(b + mid)) {

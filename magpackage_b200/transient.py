@@ -441,8 +441,8 @@ def summarize(stats) -> dict:
     return out
 
 
-def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, epochs: int = 120,
-            seed: int = 0, log=None, ideal: bool = True) -> dict:
+def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, epochs: int = 10,
+            seed: int = 0, log=None, ideal: bool = True, batch: int = 8192, lr: float = 2e-3) -> dict:
     """Plain run over all steps; train on the first half; rerun the second half learned (and ideal)."""
     from .mlp import NuPredictor
 
@@ -463,7 +463,7 @@ def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, 
         pred = NuPredictor(seed=seed)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        hist = pred.fit(feats, nu, epochs=epochs, seed=seed)
+        hist = pred.fit(feats, nu, epochs=epochs, batch=batch, lr=lr, seed=seed)
         e1.record()
         e1.synchronize()
         train_ms = e0.elapsed_time(e1)
@@ -483,7 +483,8 @@ def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, 
             "plain": summarize(plain2.stats),
             "learned": summarize(learned.stats),
             "ideal": summarize(ideal_rec.stats) if ideal else None,
-            "train": {"samples": int(feats.shape[0]), "epochs": epochs, "loss_first": hist[0],
+            "train": {"samples": int(feats.shape[0]), "epochs": epochs, "batch": batch, "lr": lr,
+                      "loss_first": hist[0],
                       "loss_last": hist[-1], "gpu_ms": train_ms},
             # the whole cost of the learned warm start on steps 101-200: its steps plus the
             # training on steps 1-100, against the plain warm start's steps
