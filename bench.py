@@ -543,8 +543,8 @@ def main():
     ap.add_argument("--instances", type=int, default=64, help="meshes of the batched_complex workload")
     ap.add_argument("--tile-variant", type=int, default=None, help="launch shape of the tile Jacobian kernel")
     ap.add_argument("--epochs", type=int, default=10, help="training epochs of the transient workload's MLP")
-    ap.add_argument("--train-batch", type=int, default=8192, help="minibatch of that training")
-    ap.add_argument("--lr", type=float, default=2e-3, help="Adam step size of that training")
+    ap.add_argument("--train-batch", type=int, default=32768, help="minibatch of that training")
+    ap.add_argument("--lr", type=float, default=4e-3, help="Adam step size of that training")
     ap.add_argument("--schedule", default="tile-blocks",
                     choices=["tile-blocks", "shared-row-blocks", "nz-row-blocks", "row-blocks", "two-pass"],
                     help="Jacobian assembly schedule (all give identical bits)")

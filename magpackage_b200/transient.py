@@ -442,7 +442,7 @@ def summarize(stats) -> dict:
 
 
 def compare(cfg: TransientConfig | None = None, train_steps: int | None = None, epochs: int = 10,
-            seed: int = 0, log=None, ideal: bool = True, batch: int = 8192, lr: float = 2e-3) -> dict:
+            seed: int = 0, log=None, ideal: bool = True, batch: int = 32768, lr: float = 4e-3) -> dict:
     """Plain run over all steps; train on the first half; rerun the second half learned (and ideal)."""
     from .mlp import NuPredictor
 

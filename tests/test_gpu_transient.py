@@ -187,7 +187,7 @@ def test_learned_warm_start_beats_plain():
     seeding with the converged nu (the bound for any predictor) does better still."""
     from magpackage_b200.transient import TransientConfig, compare
 
-    out = compare(TransientConfig(nx=20, ny=20, nz=10), epochs=120)
+    out = compare(TransientConfig(nx=20, ny=20, nz=10), epochs=120, batch=8192, lr=2e-3)
     p, l, i = out["plain"], out["learned"], out["ideal"]
     assert p["converged"] and l["converged"] and i["converged"]
     assert max(p["max_res_over_tol"], l["max_res_over_tol"], i["max_res_over_tol"]) <= 1.0
