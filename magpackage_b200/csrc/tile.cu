@@ -201,9 +201,11 @@ __device__ __forceinline__ void l2_prefetch(const void *p, size_t bytes) {
         asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((uint32_t)(hi - lo)) : "memory");
 }
 
-// What a block's next CTA visit will read first: its records (six planes), rows and chunks.
+// What a block's next CTA visit will read first: its descriptor, records (six planes), rows
+// and chunks.
 __device__ __forceinline__ void prefetch_block(const TileArgs &A, int b) {
     const TileBlock *Bp = A.blocks + b;
+    l2_prefetch(Bp, sizeof(TileBlock));
     const int rec0 = Bp->rec0, nrec = Bp->nrec;
     for (int k = 0; k < 6; k++) l2_prefetch(A.recs + (int64_t)k * A.nrec + rec0, (size_t)nrec * sizeof(uint4));
     l2_prefetch(A.rows + Bp->row0, (size_t)Bp->nrows * sizeof(uint2));

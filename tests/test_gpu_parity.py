@@ -665,6 +665,10 @@ def test_tile_schedule_shuffled_numbering_and_unused_dofs(oracle_port):
                                                                                     rt.view(torch.int64))
     v4, _ = plan.jacobian(x)
     assert torch.equal(v.view(torch.int64), v4.view(torch.int64))
+    plan.set_schedule(_lib.SCHEDULE_TWO_PASS)
+    with pytest.raises(_lib.MagError):  # the tuner is for the tile schedule only
+        plan.tune(x, vt, rt)
+    plan.set_schedule(_lib.SCHEDULE_TILE_BLOCKS)
     nu = np.random.default_rng(5).uniform(0.2, 5.0, T.shape[0]) * material.NU0
     Ik, Jk, Vk = oracle_port.curl_curl(m, nu, qw, curl)
     assert_csr_equal(plan.row_ptr, plan.col_idx, plan.stiffness(dev(nu)), oracle_matrix(oracle_port, Ik, Jk, Vk, n, False))
