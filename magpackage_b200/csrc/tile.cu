@@ -438,9 +438,11 @@ __global__ void __launch_bounds__(BT, MINB)
     for (int i = tid; i < 18 * nq; i += BT) sval[i] = __ldg(I.val_ref + i);
     for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
     __syncthreads();
-    // K pass
+    // K pass; the barrier after its last colour also tells every thread whether any element
+    // of the block conducts
     int conducting = 0;
     int c0 = 0;
+    bool any_m = false;
     for (int c = 0; c < ncolors; c++) {
         const int c1 = Bp->col_end[c];
         for (int i = c0 + tid; i < c1; i += BT) {
@@ -452,8 +454,12 @@ __global__ void __launch_bounds__(BT, MINB)
             }
         }
         c0 = c1;
-        if (c + 1 == ncolors) cp_async_wait_all();
-        __syncthreads();
+        if (c + 1 == ncolors) {
+            cp_async_wait_all();
+            any_m = __syncthreads_or(conducting) != 0;
+        } else {
+            __syncthreads();
+        }
     }
     if (ncolors == 0) {
         cp_async_wait_all();
@@ -461,7 +467,9 @@ __global__ void __launch_bounds__(BT, MINB)
     }
     tile_rows_diag<BT, true>(srows, nrows, incv, ninc, slot, nnz, A.err);
     __syncthreads();
+    // real parts; a block without a conductor stores (K, omega * 0) pairs in this one pass
     const int warp = tid >> 5, lane = tid & 31;
+    double2 *cv2 = reinterpret_cast<double2 *>(I.cvals);
     for (int c = warp; c < nchunks; c += BT / 32) {
         const uint2 ch = schunks[c];
         const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
@@ -470,29 +478,31 @@ __global__ void __launch_bounds__(BT, MINB)
             if (lane == 0) flag(A.err);
             continue;
         }
-        for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i)] = slot[sb0 + i];
+        if (any_m)
+            for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i)] = slot[sb0 + i];
+        else
+            for (int i = lane; i < len; i += 32) cv2[g + i] = make_double2(slot[sb0 + i], I.omega * 0.0);
     }
-    // block-uniform: does any element of the block conduct? (also the barrier after the stores)
-    const bool any_m = __syncthreads_or(conducting) != 0;
-    if (any_m) {
-        for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
-        __syncthreads();
-        c0 = 0;
-        for (int c = 0; c < ncolors; c++) {
-            const int c1 = Bp->col_end[c];
-            for (int i = c0 + tid; i < c1; i += BT) tile_mass_element(I, (int64_t)rec0 + i, slot, incv, nnz, ninc, sval);
-            c0 = c1;
-            __syncthreads();
-        }
-        tile_rows_diag<BT, false>(srows, nrows, incv, ninc, slot, nnz, A.err);
+    if (!any_m) return;
+    // M pass over the same slots
+    __syncthreads();  // the real parts are read out of the slots
+    for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
+    __syncthreads();
+    c0 = 0;
+    for (int c = 0; c < ncolors; c++) {
+        const int c1 = Bp->col_end[c];
+        for (int i = c0 + tid; i < c1; i += BT) tile_mass_element(I, (int64_t)rec0 + i, slot, incv, nnz, ninc, sval);
+        c0 = c1;
         __syncthreads();
     }
+    tile_rows_diag<BT, false>(srows, nrows, incv, ninc, slot, nnz, A.err);
+    __syncthreads();
     for (int c = warp; c < nchunks; c += BT / 32) {
         const uint2 ch = schunks[c];
         const int sb0 = (int)(ch.x & 0xFFFFu), len = (int)(ch.x >> 16);
         const int64_t g = (int64_t)ch.y;
         if (sb0 + len > nnz || g + len > A.nnz_total) continue;  // flagged in the K pass
-        for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i) + 1] = I.omega * (any_m ? slot[sb0 + i] : 0.0);
+        for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i) + 1] = I.omega * slot[sb0 + i];
     }
 }
 
