@@ -34,8 +34,16 @@ struct HbArgs {
     double *rscr;     // [Ne][6][2K] residual entries (re | im)
 };
 
+// Index of (r, c), r <= c, in the upper triangle of a 6 x 6 block stored row by row.
+__host__ __device__ constexpr int kb_at(int r, int c) { return r * 6 - r * (r - 1) / 2 + (c - r); }
+
+// Resident CTAs per SM the element kernel is compiled for (registers <= 65536 / (128 x this)).
+#ifndef MAG_HBFEM_MINB
+#define MAG_HBFEM_MINB 3
+#endif
+
 template <bool CALCJ>
-__global__ void __launch_bounds__(128) k_hbfem_elems(HbArgs A) {
+__global__ void __launch_bounds__(128, MAG_HBFEM_MINB) k_hbfem_elems(HbArgs A) {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= A.m.ne) return;
     const int K = A.K, N = A.N;
@@ -61,11 +69,12 @@ __global__ void __launch_bounds__(128) k_hbfem_elems(HbArgs A) {
             rr[k][h] = 0.0;
             ri[k][h] = 0.0;
         }
-    double kb[6][6];
+    // The DC block is symmetric bit for bit (C_r . C_c and C_c . C_r are the same products
+    // summed in the same order), so only its upper triangle is accumulated: kb[r][c], r <= c,
+    // at kb_at(r, c).
+    double kb[21];
 #pragma unroll
-    for (int r = 0; r < 6; r++)
-#pragma unroll
-        for (int c = 0; c < 6; c++) kb[r][c] = 0.0;
+    for (int i = 0; i < 21; i++) kb[i] = 0.0;
     const bool imag_a = A.si && A.di;
     for (int q = 0; q < A.qp.nq; q++) {
         const double w = A.qp.qw[q] * g.adet;
@@ -109,13 +118,14 @@ __global__ void __launch_bounds__(128) k_hbfem_elems(HbArgs A) {
 #pragma unroll
             for (int c = 0; c < 6; c++)
 #pragma unroll
-                for (int r = 0; r < 6; r++) {
+                for (int r = 0; r <= c; r++) {
                     const double dot = C[r][0] * C[c][0] + C[r][1] * C[c][1] + C[r][2] * C[c][2];
-                    kb[r][c] = kb[r][c] + w * nu_dc * dot;
+                    kb[kb_at(r, c)] = kb[kb_at(r, c)] + w * nu_dc * dot;
                 }
         }
     }
     double *rdst = A.rscr + (int64_t)e * 6 * 2 * K;
+#pragma unroll
     for (int i = 0; i < 6; i++) {
         const unsigned si = (sb >> i) & 1;
         for (int h = 0; h < K; h++) {
@@ -125,7 +135,7 @@ __global__ void __launch_bounds__(128) k_hbfem_elems(HbArgs A) {
         if (CALCJ) {
             double row[6];
 #pragma unroll
-            for (int j = 0; j < 6; j++) row[j] = flip(kb[i][j], si ^ ((sb >> j) & 1));
+            for (int j = 0; j < 6; j++) row[j] = flip(kb[i <= j ? kb_at(i, j) : kb_at(j, i)], si ^ ((sb >> j) & 1));
             store_row(A.scratch + e * kScratchPerElem + i * kScratchStride, row, 0.0);
         }
     }
