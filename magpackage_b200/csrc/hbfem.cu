@@ -15,8 +15,6 @@
 #include "element.cuh"
 #include "hbfem.cuh"
 
-#include <type_traits>
-
 namespace mag {
 
 namespace {
@@ -39,53 +37,44 @@ struct HbArgs {
 // Index of (r, c), r <= c, in the upper triangle of a 6 x 6 block stored row by row.
 __host__ __device__ constexpr int kb_at(int r, int c) { return r * 6 - r * (r - 1) / 2 + (c - r); }
 
-// L lanes per element (L a power of two >= K): lane h of an element's group owns
-// harmonic h. It keeps that harmonic's six signed edge values and residual accumulators in
-// registers; the time-domain edge values A_k(t) = sum_h (Re A_kh Re D(t,h) - Im A_kh Im D(t,h))
-// are summed from the lanes' terms, gathered by shuffles, in ascending h: the reference's
-// order. B(t), nu, H and the DC block are the same on every lane of the group (same inputs,
-// same operations); lane 0 keeps the DC block. No array lives in local memory.
+// Resident CTAs per SM the element kernel is compiled for (registers <= 65536 / (128 x this)).
 #ifndef MAG_HBFEM_MINB
-#define MAG_HBFEM_MINB 3  // resident CTAs per SM the element kernel is compiled for
+#define MAG_HBFEM_MINB 3
 #endif
 
-template <bool CALCJ, int L>
+template <bool CALCJ>
 __global__ void __launch_bounds__(128, MAG_HBFEM_MINB) k_hbfem_elems(HbArgs A) {
-    const int lane = threadIdx.x & 31;
-    const int sub = lane & (L - 1);
-    const int base = lane & ~(L - 1);
-    const int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / L;
-    // every lane stays to the end (the shuffles need the whole warp); an element past the
-    // end is computed on element 0's data and not stored
-    const bool valid = e < A.m.ne;
-    const int64_t ee = valid ? e : 0;
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= A.m.ne) return;
     const int K = A.K, N = A.N;
-    const bool own = sub < K;
-    const int4 tt = A.m.tet[ee];
+    const int4 tt = A.m.tet[e];
     int d[6];
-    load_dofs(A.m.dofs, ee, d);
-    const unsigned sb = A.m.signbits ? A.m.signbits[ee] : derived_signs(tt);
-    const int tag = A.m.tags[ee];
+    load_dofs(A.m.dofs, e, d);
+    const unsigned sb = A.m.signbits ? A.m.signbits[e] : derived_signs(tt);
+    const int tag = A.m.tags[e];
     Geo g;
     geometry(A.m.xyz, tt, g);
-    double arh[6], aih[6], rrh[6], rih[6];
-#pragma unroll
-    for (int k = 0; k < 6; k++) {
-        const bool has = own && d[k] >= 0;
-        const double xr = has ? __ldg(A.sr + sub * A.ndof + d[k]) : 0.0;
-        const double xi = has && A.si ? __ldg(A.si + sub * A.ndof + d[k]) : 0.0;
-        arh[k] = flip(xr, (sb >> k) & 1);
-        aih[k] = flip(xi, (sb >> k) & 1);
-        rrh[k] = 0.0;
-        rih[k] = 0.0;
-    }
+    double ar[6][kMaxHarm], ai[6][kMaxHarm];
+    for (int k = 0; k < 6; k++)
+        for (int h = 0; h < K; h++) {
+            const bool has = d[k] >= 0;
+            const double xr = has ? __ldg(A.sr + h * A.ndof + d[k]) : 0.0;
+            const double xi = has && A.si ? __ldg(A.si + h * A.ndof + d[k]) : 0.0;
+            ar[k][h] = flip(xr, (sb >> k) & 1);
+            ai[k][h] = flip(xi, (sb >> k) & 1);
+        }
+    double rr[6][kMaxHarm], ri[6][kMaxHarm];
+    for (int k = 0; k < 6; k++)
+        for (int h = 0; h < K; h++) {
+            rr[k][h] = 0.0;
+            ri[k][h] = 0.0;
+        }
     // The DC block is symmetric bit for bit (C_r . C_c and C_c . C_r are the same products
     // summed in the same order), so only its upper triangle is accumulated: kb[r][c], r <= c,
-    // at kb_at(r, c), in shared memory (lane 0 of the group owns its element's 21 entries).
-    __shared__ double kbs[128 / L][21];
-    double *kb = kbs[threadIdx.x / L];
-    if (CALCJ && sub == 0)
-        for (int i = 0; i < 21; i++) kb[i] = 0.0;
+    // at kb_at(r, c).
+    double kb[21];
+#pragma unroll
+    for (int i = 0; i < 21; i++) kb[i] = 0.0;
     const bool imag_a = A.si && A.di;
     for (int q = 0; q < A.qp.nq; q++) {
         const double w = A.qp.qw[q] * g.adet;
@@ -93,15 +82,14 @@ __global__ void __launch_bounds__(128, MAG_HBFEM_MINB) k_hbfem_elems(HbArgs A) {
         curls_generic(g, A.qp.curl_ref, q, C);
         double sum_nu = 0.0;
         for (int t = 0; t < N; t++) {
-            const double drh = own ? __ldg(A.dr + sub * N + t) : 0.0;
-            const double dih = own && imag_a ? __ldg(A.di + sub * N + t) : 0.0;
             double at[6];
-#pragma unroll
             for (int k = 0; k < 6; k++) {
-                double term = arh[k] * drh;
-                if (imag_a) term = term - aih[k] * dih;
                 double acc = 0.0;
-                for (int h = 0; h < K; h++) acc = acc + __shfl_sync(0xFFFFFFFFu, term, base + h);
+                for (int h = 0; h < K; h++) {
+                    double term = ar[k][h] * __ldg(A.dr + h * N + t);
+                    if (imag_a) term = term - ai[k][h] * __ldg(A.di + h * N + t);
+                    acc = acc + term;
+                }
                 at[k] = acc;
             }
             double B[3] = {0.0, 0.0, 0.0};
@@ -114,20 +102,20 @@ __global__ void __launch_bounds__(128, MAG_HBFEM_MINB) k_hbfem_elems(HbArgs A) {
             material_eval(A.mp, tag, bsq, nu, dnu);
             sum_nu = sum_nu + nu;
             const double H[3] = {nu * B[0], nu * B[1], nu * B[2]};
-            if (own) {
-                const double p_r = __ldg(A.pr + t * K + sub);
-                const double p_i = A.pi ? __ldg(A.pi + t * K + sub) : 0.0;
+            for (int h = 0; h < K; h++) {
+                const double p_r = __ldg(A.pr + t * K + h);
+                const double p_i = A.pi ? __ldg(A.pi + t * K + h) : 0.0;
 #pragma unroll
                 for (int i = 0; i < 6; i++) {
                     const double dot = C[i][0] * H[0] + C[i][1] * H[1] + C[i][2] * H[2];
-                    rrh[i] = rrh[i] + w * dot * p_r;
-                    if (A.pi) rih[i] = rih[i] + w * dot * p_i;
+                    rr[i][h] = rr[i][h] + w * dot * p_r;
+                    if (A.pi) ri[i][h] = ri[i][h] + w * dot * p_i;
                 }
             }
         }
-        if (CALCJ && sub == 0) {
+        if (CALCJ) {
             const double nu_dc = sum_nu / (double)N;
-#pragma unroll 1
+#pragma unroll
             for (int c = 0; c < 6; c++)
 #pragma unroll
                 for (int r = 0; r <= c; r++) {
@@ -136,16 +124,15 @@ __global__ void __launch_bounds__(128, MAG_HBFEM_MINB) k_hbfem_elems(HbArgs A) {
                 }
         }
     }
-    if (!valid) return;
-    double *rdst = A.rscr + e * 6 * 2 * K;
+    double *rdst = A.rscr + (int64_t)e * 6 * 2 * K;
 #pragma unroll
     for (int i = 0; i < 6; i++) {
         const unsigned si = (sb >> i) & 1;
-        if (own) {
-            rdst[i * 2 * K + sub] = flip(rrh[i], si);
-            rdst[i * 2 * K + K + sub] = flip(rih[i], si);
+        for (int h = 0; h < K; h++) {
+            rdst[i * 2 * K + h] = flip(rr[i][h], si);
+            rdst[i * 2 * K + K + h] = flip(ri[i][h], si);
         }
-        if (CALCJ && sub == 0) {
+        if (CALCJ) {
             double row[6];
 #pragma unroll
             for (int j = 0; j < 6; j++) row[j] = flip(kb[i <= j ? kb_at(i, j) : kb_at(j, i)], si ^ ((sb >> j) & 1));
@@ -178,20 +165,10 @@ int launch_hbfem(const ElemData &m, const RowPlan &rp, int max_row, const double
                  const double *dr, const double *di, const double *pr, const double *pi, int N,
                  const QuadParams &qp, const MaterialParams &mp, double *scratch, double *rscr, double *vals,
                  double *out_re, double *out_im, cudaStream_t s) {
-    if (K < 1 || K > kMaxHarm) return MAG_E_ARG;
     HbArgs A{m, sr, si, dr, di, pr, pi, K, N, rp.ndof, qp, mp, vals ? scratch : nullptr, rscr};
-    const int L = K == 1 ? 1 : K == 2 ? 2 : K <= 4 ? 4 : K <= 8 ? 8 : 16;  // lanes per element
-    const unsigned g = (unsigned)((m.ne * L + 127) / 128);
-    auto go = [&](auto calcj, auto lanes) { k_hbfem_elems<decltype(calcj)::value, decltype(lanes)::value><<<g, 128, 0, s>>>(A); };
-    using T = std::true_type;
-    using F = std::false_type;
-    switch (L) {
-        case 1: vals ? go(T{}, std::integral_constant<int, 1>{}) : go(F{}, std::integral_constant<int, 1>{}); break;
-        case 2: vals ? go(T{}, std::integral_constant<int, 2>{}) : go(F{}, std::integral_constant<int, 2>{}); break;
-        case 4: vals ? go(T{}, std::integral_constant<int, 4>{}) : go(F{}, std::integral_constant<int, 4>{}); break;
-        case 8: vals ? go(T{}, std::integral_constant<int, 8>{}) : go(F{}, std::integral_constant<int, 8>{}); break;
-        default: vals ? go(T{}, std::integral_constant<int, 16>{}) : go(F{}, std::integral_constant<int, 16>{}); break;
-    }
+    const unsigned g = (unsigned)((m.ne + 127) / 128);
+    if (vals) k_hbfem_elems<true><<<g, 128, 0, s>>>(A);
+    else k_hbfem_elems<false><<<g, 128, 0, s>>>(A);
     if (cudaPeekAtLastError() != cudaSuccess) return MAG_E_CUDA;
     const int64_t nt = rp.ndof * 2 * K;
     k_rows_reduce_harm<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(rp, rscr, K, out_re, out_im);
