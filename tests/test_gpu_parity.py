@@ -440,6 +440,45 @@ def test_batched_complex_matches_oracle(oracle_port):
     batch.close()
 
 
+def test_batched_complex_unit_sigma_and_negative_omega(oracle_port):
+    """A mesh without sigma (sigma = 1: every block conducts and takes the M pass) and
+    non-uniform quadrature weights (the kernels' general per-point sums), one whose conductor
+    covers only a few blocks, and a negative omega: every variant equals the oracle bit for bit."""
+    from magpackage_b200.plan import ComplexBatch
+
+    qw4, val, curl = quadrature.reference_data(2)
+    plans, nus, sigmas, refs, omegas = [], [], [], [], []
+    for k, (nx, ny, nz) in enumerate(((6, 5, 4), (11, 9, 8))):
+        mesh = synth.kuhn_box(nx, ny, nz, seed=11 + k)
+        tags = synth.cube_layout(mesh)
+        edges, t2e, sign, m = make_case(oracle_port, mesh.P, mesh.T, tags)
+        E = edges.shape[0]
+        rng = np.random.default_rng(20 + k)
+        nu = rng.uniform(0.5, 2.0, mesh.num_elements) * material.NU0
+        sigma = None if k == 0 else np.where(tags == synth.IRON, 1e6, 0.0)
+        qw = np.array([0.05, 0.04, 0.045, 0.0316666]) if k == 0 else qw4
+        I, J, Vk = oracle_port.curl_curl(m, nu, qw, curl)
+        _, _, Vm = oracle_port.mass(m, np.ones(mesh.num_elements) if sigma is None else sigma, qw, val)
+        plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
+        plan.set_quadrature(qw, curl, val)
+        plans.append(plan)
+        nus.append(dev(nu))
+        sigmas.append(None if sigma is None else dev(sigma))
+        omegas.append(-2 * np.pi * 60.0 if k == 1 else 2 * np.pi * 400.0)
+        refs.append((oracle_matrix(oracle_port, I, J, Vk, E, False), oracle_matrix(oracle_port, I, J, Vm, E, False)))
+    batch = ComplexBatch(plans, nus, sigmas, omegas)
+    _, times, _ = batch.tuning()
+    assert np.all(times > 0)
+    for variant in range(len(times)):
+        batch.select(variant)
+        vals = batch.assemble()
+        torch.cuda.synchronize()
+        for plan, v, (kref, mref), omega in zip(plans, vals, refs, omegas):
+            assert_csr_equal(plan.row_ptr, plan.col_idx, v.real.contiguous(), kref)
+            assert bits_equal(host(v.imag.contiguous()), omega * mref[2]), variant
+    batch.close()
+
+
 def test_batched_complex_slot_and_row_paths(oracle_port):
     """A batch mixing a mesh whose off-diagonal entries have at most two contributions (slot
     path), one where a dof shared by two edges breaks that bound (row phase) and one with
