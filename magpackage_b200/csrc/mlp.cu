@@ -648,6 +648,13 @@ int mlp_forward(const MlpForwardArgs &a, int grid, cudaStream_t s) {
     size_t sm = sizeof(Smem);
     auto kern = a.z_out ? k_mlp_forward<false> : k_mlp_forward<true>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    // The CTAs loop over tiles: no more CTAs than fit at once, so that none starts after
+    // the others have finished their share (a second, thin wave).
+    int dev = 0, nsm = 0, per = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kRows, sm) == cudaSuccess && per > 0 &&
+        grid > per * nsm)
+        grid = per * nsm;
     kern<<<grid, kRows, sm, s>>>(a);
     return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
 }
