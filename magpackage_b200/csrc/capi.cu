@@ -1173,7 +1173,7 @@ int mag_mlp_forward(mag_mlp *n, const float *d_feats, int64_t rows, float *d_y, 
     }
     MlpForwardArgs a{d_feats, rows, n->params, n->ops, d_y, d_z, nullptr, nullptr, 0, 0, 0, 0, n->err,
                      n->spin_limit};
-    return mlp_forward(a, mlp_grid(rows, 4 * n->grid), (cudaStream_t)stream);
+    return mlp_forward(a, mlp_grid(rows, 1 << 30), (cudaStream_t)stream);
 }
 
 int mag_mlp_predict_nu(mag_mlp *n, const float *d_feats, int64_t rows, const int32_t *d_rows, double y_scale,
@@ -1184,7 +1184,7 @@ int mag_mlp_predict_nu(mag_mlp *n, const float *d_feats, int64_t rows, const int
     }
     MlpForwardArgs a{d_feats, rows, n->params, n->ops, nullptr, nullptr, d_nu, d_rows, y_scale, y_shift,
                      nu_min, nu_max, n->err, n->spin_limit};
-    return mlp_forward(a, mlp_grid(rows, 4 * n->grid), (cudaStream_t)stream);
+    return mlp_forward(a, mlp_grid(rows, 1 << 30), (cudaStream_t)stream);
 }
 
 int mag_mlp_gradient(mag_mlp *n, const float *d_feats, const float *d_target, int64_t rows, float loss_scale,
@@ -1196,7 +1196,7 @@ int mag_mlp_gradient(mag_mlp *n, const float *d_feats, const float *d_target, in
     cudaStream_t s = (cudaStream_t)stream;
     MlpForwardArgs fa{d_feats, rows, n->params, n->ops, d_y, d_z, nullptr, nullptr, 0, 0, 0, 0, n->err,
                       n->spin_limit};
-    MAG_TRY(mlp_forward(fa, mlp_grid(rows, 4 * n->grid), s));
+    MAG_TRY(mlp_forward(fa, mlp_grid(rows, 1 << 30), s));
     MlpBackwardArgs ba{d_feats, d_z, d_y, d_target, rows, loss_scale, n->params, n->ops, n->partial,
                        d_grad ? d_grad : n->grad, n->err, n->spin_limit};
     return mlp_backward(ba, mlp_grid(rows, n->grid), s);
