@@ -291,6 +291,14 @@ int mag_mlp_gradient(mag_mlp *mlp, const float *d_feats, const float *d_target, 
 /* One Adam step (lr, betas 0.9/0.999) on the mean-squared error of a minibatch. */
 int mag_mlp_train_step(mag_mlp *mlp, const float *d_feats, const float *d_target, int64_t rows,
                        float lr, float *d_y, float *d_z, void *stream);
+/* One epoch of mag_mlp_train_step over minibatches of `batch` rows in the order of the
+ * device permutation d_perm [rows] (a last partial minibatch is skipped): each minibatch is
+ * gathered on the device into d_xb [batch][4] and d_tb [batch] (16-byte aligned), so the
+ * host only enqueues launches. d_loss (or NULL) accumulates the sum of squared errors of
+ * every minibatch before its step. d_y [batch], d_z [batch][3][64] are workspace. */
+int mag_mlp_train_epoch(mag_mlp *mlp, const float *d_feats, const float *d_target, int64_t rows,
+                        const int64_t *d_perm, int64_t batch, float lr, float *d_xb, float *d_tb, float *d_y,
+                        float *d_z, float *d_loss, void *stream);
 /* Synchronise; MAG_E_TIMEOUT if a tensor-core completion wait gave up since the last
  * check (the status is cleared once reported). The outputs of that call are incomplete. */
 int mag_mlp_check(mag_mlp *mlp, void *stream);

@@ -85,6 +85,7 @@ _PROTOS = {
                            _int),
     "mag_mlp_gradient": ([_vp, _vp, _vp, _i64, C.c_float, _vp, _vp, _vp, _vp], _int),
     "mag_mlp_train_step": ([_vp, _vp, _vp, _i64, C.c_float, _vp, _vp, _vp], _int),
+    "mag_mlp_train_epoch": ([_vp, _vp, _vp, _i64, _vp, _i64, C.c_float, _vp, _vp, _vp, _vp, _vp, _vp], _int),
     "mag_mlp_check": ([_vp, _vp], _int),
     "mag_mlp_set_spin_limit": ([_vp, _i64], _int),
     "mag_csr_drop_zeros": ([_vp, _vp, _vp, _i64, _vp, _vp, _vp, C.POINTER(_i64), _vp], _int),

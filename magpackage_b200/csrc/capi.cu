@@ -1211,6 +1211,23 @@ int mag_mlp_train_step(mag_mlp *n, const float *d_feats, const float *d_target, 
     return mlp_pack(n->params, n->ops, s);
 }
 
+int mag_mlp_train_epoch(mag_mlp *n, const float *d_feats, const float *d_target, int64_t rows,
+                        const int64_t *d_perm, int64_t batch, float lr, float *d_xb, float *d_tb, float *d_y,
+                        float *d_z, float *d_loss, void *stream) {
+    if (!n || !d_feats || !d_target || !d_perm || rows <= 0 || batch <= 0 || !d_xb || !d_tb || !d_y || !d_z ||
+        ((uintptr_t)d_feats & 15) || ((uintptr_t)d_xb & 15)) {
+        set_error("mag_mlp_train_epoch: bad arguments");
+        return MAG_E_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int64_t off = 0; off + batch <= rows; off += batch) {
+        MAG_TRY(mlp_gather(d_feats, d_target, d_perm, off, batch, d_xb, d_tb, s));
+        MAG_TRY(mag_mlp_train_step(n, d_xb, d_tb, batch, lr, d_y, d_z, stream));
+        if (d_loss) MAG_TRY(mlp_sqerr(d_y, d_tb, batch, d_loss, s));
+    }
+    return MAG_OK;
+}
+
 int mag_mlp_check(mag_mlp *n, void *stream) {
     if (!n) return MAG_E_ARG;
     int h = 0;

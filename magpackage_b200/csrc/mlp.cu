@@ -634,7 +634,47 @@ __global__ void k_mlp_pack(const float *__restrict__ P, __nv_bfloat16 *__restric
     }
 }
 
+__global__ void k_mlp_gather(const float4 *__restrict__ feats, const float *__restrict__ target,
+                             const int64_t *__restrict__ perm, int64_t off, int64_t b, float4 *__restrict__ xb,
+                             float *__restrict__ tb) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= b) return;
+    const int64_t r = perm[off + i];
+    xb[i] = feats[r];
+    tb[i] = target[r];
+}
+
+// One CTA of 1024 threads: strided partial sums, then a fixed tree over the shared array.
+__global__ void __launch_bounds__(1024) k_mlp_sqerr(const float *__restrict__ y, const float *__restrict__ t,
+                                                    int64_t b, float *__restrict__ acc) {
+    __shared__ float part[1024];
+    float v = 0.0f;
+    for (int64_t i = threadIdx.x; i < b; i += 1024) {
+        const float d = y[i] - t[i];
+        v += d * d;
+    }
+    part[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = 512; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *acc += part[0];
+}
+
 }  // namespace
+
+int mlp_gather(const float *feats, const float *target, const int64_t *perm, int64_t off, int64_t b, float *xb,
+               float *tb, cudaStream_t s) {
+    k_mlp_gather<<<(unsigned)((b + 255) / 256), 256, 0, s>>>(reinterpret_cast<const float4 *>(feats), target, perm,
+                                                            off, b, reinterpret_cast<float4 *>(xb), tb);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
+
+int mlp_sqerr(const float *y, const float *t, int64_t b, float *acc, cudaStream_t s) {
+    k_mlp_sqerr<<<1, 1024, 0, s>>>(y, t, b, acc);
+    return cudaPeekAtLastError() == cudaSuccess ? MAG_OK : MAG_E_CUDA;
+}
 
 size_t mlp_forward_smem() { return sizeof(Smem) + 1024; }
 size_t mlp_backward_smem() { return sizeof(BwdSmem) + 1024; }

@@ -46,5 +46,10 @@ int mlp_forward(const MlpForwardArgs &a, int grid, cudaStream_t s);
 int mlp_backward(const MlpBackwardArgs &a, int grid, cudaStream_t s);
 int mlp_adam(float *params, const float *grad, float *m, float *v, float lr, float b1, float b2, float eps,
              int step, cudaStream_t s);
+// xb[i] = feats[perm[off + i]] (16-byte rows), tb[i] = target[perm[off + i]], i < b.
+int mlp_gather(const float *feats, const float *target, const int64_t *perm, int64_t off, int64_t b, float *xb,
+               float *tb, cudaStream_t s);
+// *acc += sum_i (y_i - t_i)^2 over i < b, in a fixed order (one CTA).
+int mlp_sqerr(const float *y, const float *t, int64_t b, float *acc, cudaStream_t s);
 
 }  // namespace mag

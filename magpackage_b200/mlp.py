@@ -83,6 +83,13 @@ class MLP:
                                                 _ptr(y), _ptr(z), _lib.stream_ptr()))
         return y
 
+    def train_epoch(self, feats, target, perm, batch: int, lr: float, xb, tb, y, z, loss=None):
+        """One epoch of train_step over minibatches in the order of the device permutation
+        perm (int64); the minibatches are gathered on the device (mag_mlp_train_epoch)."""
+        _lib.check(self._lib.mag_mlp_train_epoch(self._h, _ptr(feats), _ptr(target), feats.shape[0], _ptr(perm),
+                                                 int(batch), C.c_float(lr), _ptr(xb), _ptr(tb), _ptr(y), _ptr(z),
+                                                 _ptr(loss), _lib.stream_ptr()))
+
     def predict_nu(self, feats, rows, nu_out, y_scale, y_shift, nu_min, nu_max):
         n = feats.shape[0]
         _lib.check(self._lib.mag_mlp_predict_nu(self._h, _ptr(feats), n, _ptr(rows), y_scale, y_shift, nu_min,
@@ -132,25 +139,22 @@ class NuPredictor:
         xn = self._norm(feats)
         tn = ((ly - self.y_mean) / self.y_std).float().contiguous()
         n = xn.shape[0]
-        # permutations drawn on the device and the loss summed there: no host round trip
-        # per minibatch, so the steps run back to back on the GPU
+        # permutations drawn on the device, minibatches gathered and the loss summed there:
+        # the host only enqueues launches, and the steps run back to back on the GPU
         g = torch.Generator(device="cuda")
         g.manual_seed(seed)
-        hist = []
+        batch = min(batch, n)
         ybuf = torch.empty(batch, dtype=torch.float32, device="cuda")
         zbuf = torch.empty((batch, 3, 64), dtype=torch.float32, device="cuda")
-        steps = max(1, n // batch)
+        xb = torch.empty((batch, 4), dtype=torch.float32, device="cuda")
+        tb = torch.empty(batch, dtype=torch.float32, device="cuda")
+        loss = torch.zeros(epochs, dtype=torch.float32, device="cuda")
         for ep in range(epochs):
             perm = torch.randperm(n, generator=g, device="cuda")
-            tot = torch.zeros((), dtype=torch.float32, device="cuda")
-            for i in range(0, n - batch + 1, batch):
-                idx = perm[i:i + batch]
-                xb, tb = xn[idx].contiguous(), tn[idx].contiguous()
-                y = self.mlp.train_step(xb, tb, lr, ybuf, zbuf)
-                tot += ((y - tb) ** 2).mean()
-            hist.append(tot)
+            self.mlp.train_epoch(xn, tn, perm, batch, lr, xb, tb, ybuf, zbuf, loss[ep:ep + 1])
         self.mlp.check()
-        return [float(h) / steps for h in hist]
+        # mean squared error per row of each epoch (before each minibatch's step)
+        return (loss.double() / ((n // batch) * batch)).tolist()
 
     def predict_nu(self, feats: torch.Tensor, rows: torch.Tensor, nu_out: torch.Tensor, nu_min: float,
                    nu_max: float):

@@ -89,3 +89,31 @@ def test_bounded_wait_gives_up_and_recovers():
     net.check()  # the status was cleared when it was reported
     y_ref, _ = mlp_ref.forward(p, x)
     assert np.max(np.abs(y.cpu().numpy() - y_ref)) <= 2e-3 * (1 + np.max(np.abs(y_ref)))
+
+
+def test_train_epoch_equals_train_steps():
+    """mag_mlp_train_epoch (minibatches gathered on the device in the permutation's order)
+    leaves the same parameters, bit for bit, as train_step on host-gathered minibatches; its
+    loss sum is the minibatches' squared errors."""
+    rng = np.random.default_rng(4)
+    n, batch = 10000, 2048
+    x = torch.as_tensor(rng.normal(0, 1, (n, 4)).astype(np.float32), device="cuda")
+    t = torch.as_tensor(rng.normal(0, 1, n).astype(np.float32), device="cuda")
+    perm = torch.as_tensor(rng.permutation(n), dtype=torch.int64, device="cuda")
+    a, b = MLP(init_params(5)), MLP(init_params(5))
+    y = torch.empty(batch, dtype=torch.float32, device="cuda")
+    z = torch.empty((batch, 3, 64), dtype=torch.float32, device="cuda")
+    xb = torch.empty((batch, 4), dtype=torch.float32, device="cuda")
+    tb = torch.empty(batch, dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    a.train_epoch(x, t, perm, batch, 3e-3, xb, tb, y, z, loss)
+    a.check()
+    ref = 0.0
+    for i in range(0, n - batch + 1, batch):
+        idx = perm[i:i + batch]
+        xi, ti = x[idx].contiguous(), t[idx].contiguous()
+        yi = b.train_step(xi, ti, 3e-3)
+        ref += float(((yi - ti) ** 2).sum())
+    b.check()
+    assert np.array_equal(a.params().view(np.int32), b.params().view(np.int32))
+    assert abs(float(loss[0]) - ref) <= 1e-4 * ref
