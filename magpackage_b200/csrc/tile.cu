@@ -152,6 +152,12 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
         const unsigned s = sl[l];
         if (s == kTileAbsent) continue;
         const int nzb = (int)(s & 0xFFFFu), is = (int)(s >> 16);
+        // One check per row: the slot region has kTileSlotPad doubles beyond the largest
+        // block, so nzb < bnnz keeps every nzb + p (p <= 30) inside it.
+        if (nzb >= bnnz) {
+            flag(A.err);
+            continue;
+        }
         const unsigned si = (sb >> l) & 1u;
         const double rv = STIFF ? 0.0 : flip(qsum4<Q4>(nu * b[l], A.qp, w0, adet), si);
         double dv = 0.0;
@@ -180,8 +186,7 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
                 const unsigned p = (pos[l] >> (5 * j)) & 31u;
                 if (p == (unsigned)kCompactMaxRow) continue;
                 const int k = nzb + (int)p;
-                if (k < bnnz) slot[k] = slot[k] + flip(v[j], si ^ ((sb >> j) & 1u));
-                else flag(A.err);
+                slot[k] = slot[k] + flip(v[j], si ^ ((sb >> j) & 1u));
             }
         }
         if (is < binc) {
@@ -240,7 +245,7 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int 
         const int nrows = Bp->nrows, row0 = Bp->row0, rec0 = Bp->rec0, nrec = Bp->nrec;
         const int nnz = Bp->nnz, ninc = Bp->ninc, ncolors = Bp->ncolors;
         const int chunk0 = Bp->chunk0, nchunks = Bp->nchunks;
-        if (nrows > A.smem_rows || nchunks > A.smem_chunks || nnz > A.smem_nnz || ninc > A.smem_inc) {
+        if (nrows > A.smem_rows || nchunks > A.smem_chunks || nnz > A.smem_nnz - kTileSlotPad || ninc > A.smem_inc) {
             if (tid == 0) flag(A.err);  // the whole CTA leaves before its first barrier
             return;
         }
@@ -348,6 +353,10 @@ __device__ __forceinline__ void tile_mass_element(const TileComplexInstance &I, 
         const unsigned s = sl[l];
         if (s == kTileAbsent) continue;
         const int nzb = (int)(s & 0xFFFFu), is = (int)(s >> 16);
+        if (nzb >= bnnz) {  // one check per row (kTileSlotPad)
+            flag(A.err);
+            continue;
+        }
         const unsigned si = (sb >> l) & 1u;
         double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll 1
@@ -371,8 +380,7 @@ __device__ __forceinline__ void tile_mass_element(const TileComplexInstance &I, 
             const unsigned p = (pos[l] >> (5 * j)) & 31u;
             if (p == (unsigned)kCompactMaxRow) continue;
             const int k = nzb + (int)p;
-            if (k < bnnz) slot[k] = slot[k] + flip(m[j], si ^ ((sb >> j) & 1u));
-            else flag(A.err);
+            slot[k] = slot[k] + flip(m[j], si ^ ((sb >> j) & 1u));
         }
         if (is < binc) incv[is].x = m[l];  // the diagonal: si ^ si = 0, no flip
         else flag(A.err);
@@ -428,7 +436,8 @@ __global__ void __launch_bounds__(BT, MINB)
     const int nnz = Bp->nnz, ninc = Bp->ninc, ncolors = Bp->ncolors;
     const int chunk0 = Bp->chunk0, nchunks = Bp->nchunks;
     const int nq = A.qp.nq;
-    if (nrows > smem_rows || nchunks > smem_chunks || nnz > smem_nnz || ninc > smem_inc || nq > kMaxQuad) {
+    if (nrows > smem_rows || nchunks > smem_chunks || nnz > smem_nnz - kTileSlotPad || ninc > smem_inc ||
+        nq > kMaxQuad) {
         if (tid == 0) flag(A.err);  // the whole CTA leaves before its first barrier
         return;
     }
@@ -990,7 +999,7 @@ namespace {
 // Shared memory of one CTA: the block's values (an even count of doubles), the incidence
 // slots (double2), then the block's row table and store chunks (uint2 each).
 size_t tile_smem_bytes(const TilePlan &tp, TileArgs *a) {
-    a->smem_nnz = (tp.max_nnz + 1) & ~1;
+    a->smem_nnz = ((tp.max_nnz + 1) & ~1) + kTileSlotPad;
     a->smem_inc = tp.max_inc;
     a->smem_rows = tp.max_rows;
     a->smem_chunks = tp.max_chunks;
@@ -1118,7 +1127,7 @@ int build_tile_complex(const std::vector<TileComplexInput> &in, TileComplexBatch
         t.val_ref = in[i].qp.val_ref;
         t.omega = in[i].omega;
         t.cvals = in[i].vals;
-        b->smem_nnz = std::max(b->smem_nnz, (tp.max_nnz + 1) & ~1);
+        b->smem_nnz = std::max(b->smem_nnz, ((tp.max_nnz + 1) & ~1) + kTileSlotPad);
         b->smem_inc = std::max(b->smem_inc, tp.max_inc);
         b->smem_rows = std::max(b->smem_rows, tp.max_rows);
         b->smem_chunks = std::max(b->smem_chunks, tp.max_chunks);

@@ -14,6 +14,8 @@ constexpr int kTileMaxNnz = 8191;   // CSR nonzeros per block (13-bit offsets in
 constexpr int kTileMaxInc = 4095;   // (row, element) incidences per block (12-bit offsets)
 constexpr int kTileMaxColors = 8;   // element colour classes per block
 constexpr int kTileChunk = 256;     // nonzeros per store chunk (one warp stores a chunk)
+constexpr int kTileSlotPad = 32;    // doubles of slack after a block's values in shared memory (even):
+                                    // a row's first nonzero plus any 5-bit position stays inside
 constexpr int kTileVariants = 4;    // launch shapes of the Jacobian kernel (tile_variant_name)
 constexpr int kTileDepths = 3;      // L2 staging depths, in waves of resident CTAs (0, 1, 2)
 constexpr uint32_t kTileAbsent = 0xFFFFFFFFu;
