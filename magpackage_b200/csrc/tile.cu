@@ -183,9 +183,7 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
 #pragma unroll
             for (int j = 0; j < 6; j++) {
                 if (j == l) continue;
-                const unsigned p = (pos[l] >> (5 * j)) & 31u;
-                if (p == (unsigned)kCompactMaxRow) continue;
-                const int k = nzb + (int)p;
+                const int k = nzb + (int)((pos[l] >> (5 * j)) & 31u);  // absent column: the diagonal
                 slot[k] = slot[k] + flip(v[j], si ^ ((sb >> j) & 1u));
             }
         }
@@ -377,9 +375,7 @@ __device__ __forceinline__ void tile_mass_element(const TileComplexInstance &I, 
 #pragma unroll
         for (int j = 0; j < 6; j++) {
             if (j == l) continue;
-            const unsigned p = (pos[l] >> (5 * j)) & 31u;
-            if (p == (unsigned)kCompactMaxRow) continue;
-            const int k = nzb + (int)p;
+            const int k = nzb + (int)((pos[l] >> (5 * j)) & 31u);  // absent column: the diagonal
             slot[k] = slot[k] + flip(m[j], si ^ ((sb >> j) & 1u));
         }
         if (is < binc) incv[is].x = m[l];  // the diagonal: si ^ si = 0, no flip
@@ -794,6 +790,19 @@ bool plan_tiles_host(const TileHostMesh &hm, TileHostPlan *out) {
                 }
             }
             if (fail) continue;
+            // An absent column (a dof of -1) of a row points at the row's own diagonal
+            // nonzero: the kernels add its discarded value there without a test, and the row
+            // phase overwrites that slot with the diagonal's element-ordered sum afterwards.
+            for (int32_t i = 0; i < nr; i++) {
+                HostRec &h = rec[i];
+                for (int l = 0; l < 6; l++) {
+                    if (h.w[18 + l] == kTileAbsent) continue;
+                    const uint32_t diagp = (h.w[12 + l] >> (5 * l)) & 31u;
+                    for (int j = 0; j < 6; j++)
+                        if (((h.w[12 + l] >> (5 * j)) & 31u) == (uint32_t)kCompactMaxRow)
+                            h.w[12 + l] = (h.w[12 + l] & ~(31u << (5 * j))) | (diagp << (5 * j));
+                }
+            }
             // adjacency (CSR over records)
             adj_ptr.assign((size_t)nr + 1, 0);
             for (int32_t sl = 0; sl < bn; sl++)

@@ -38,7 +38,8 @@ static_assert(sizeof(TileBlock) == 80, "TileBlock layout");
 //   plane 0: tet (4 node ids)
 //   plane 1: dofs 0..3
 //   plane 2: dofs 4, 5, element id, tag | sign bits << 8
-//   plane 3: per local row 0..3 its six 5-bit in-row column positions (31 = no dof)
+//   plane 3: per local row 0..3 its six 5-bit in-row column positions (a column without a
+//            dof holds the row's diagonal position: the value added there is overwritten)
 //   plane 4: positions of local rows 4, 5; slots of local rows 0, 1
 //   plane 5: slots of local rows 2..5
 // where a slot is (row's first nonzero in the block) | (incidence slot << 16), or

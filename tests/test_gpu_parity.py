@@ -645,6 +645,34 @@ def test_stiffness_nonzero_pass_matches_oracle(oracle_port):
             assert torch.equal(plan.stiffness(dev(nu)), k_nz)
 
 
+def test_tile_schedule_absent_dofs(oracle_port):
+    """Edges without a dof (-1, as DofHandler gives outside the target regions) on the tile
+    schedule: the absent columns' values go to the row's diagonal slot, which the row phase
+    overwrites; Jacobian, residual and K(nu) equal the oracle bit for bit."""
+    mesh = synth.kuhn_box(10, 9, 8, seed=6)
+    tags = synth.cube_layout(mesh)
+    edges, t2e, sign = oracle_port.generate_edges(mesh.T)
+    E = edges.shape[0]
+    dofs = np.where(t2e % 5 == 3, -1, t2e).astype(np.int32)
+    m = mex_inputs(mesh.P, mesh.T, dofs, sign, tags)
+    sol = np.random.default_rng(3).normal(0, 0.05, E)
+    qw, val, curl = quadrature.reference_data(2)
+    pk = material.pack_material_data(synth.standard_materials())
+    plan = AssemblyPlan(mesh.P, mesh.T, dofs, E, tags, sign)
+    plan.set_materials(pk)
+    assert plan.info.schedule == _lib.SCHEDULE_TILE_BLOCKS
+    I, J, V, Ri, Rv = oracle_port.jacobian(m, sol, qw, curl, pk, True)
+    v, r = plan.jacobian(dev(sol))
+    plan.check()
+    assert_csr_equal(plan.row_ptr, plan.col_idx, v, oracle_matrix(oracle_port, I, J, V, E, False))
+    assert bits_equal(host(r), oracle_port.sparse_vec(Ri, Rv, E))
+    nu = np.random.default_rng(4).uniform(0.2, 5.0, mesh.num_elements) * material.NU0
+    Ik, Jk, Vk = oracle_port.curl_curl(m, nu, qw, curl)
+    assert_csr_equal(plan.row_ptr, plan.col_idx, plan.stiffness(dev(nu)), oracle_matrix(oracle_port, Ik, Jk, Vk, E, False))
+    plan.check()
+    plan.close()
+
+
 def test_tile_schedule_shuffled_numbering_and_unused_dofs(oracle_port):
     """The tile schedule on a mesh whose node and element numbering is shuffled (a block's
     rows are then scattered over the CSR in short runs) with three unused dofs at the end
