@@ -114,6 +114,18 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
     geometry(A.xyz, tt, g);
     double C[6][3];
     curls_standard(g, C);
+    // Orientation signs folded into the curls (C_j s_j): negation is exact and commutes with
+    // rounding to nearest, so B = sum a_j C_j is the same bits with unsigned edge values, and
+    // every entry below comes out as s_l s_j times the unsigned one, which is how the
+    // reference signs its finished entries. Only the sign of an exact zero can differ, and
+    // every sum these entries enter starts from +0, which absorbs it.
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+        if ((sb >> j) & 1u) {
+            C[j][0] = -C[j][0];
+            C[j][1] = -C[j][1];
+            C[j][2] = -C[j][2];
+        }
     constexpr bool STIFF = MODE == kStiffness;
     double nu, g2 = 0.0, b[6];
     double nut = 0.0, be = 1.0;  // seeded tangent: nu(|beta B|^2), beta
@@ -125,7 +137,7 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
         const int d[6] = {(int)p1.x, (int)p1.y, (int)p1.z, (int)p1.w, (int)p2.x, (int)p2.y};
         double a[6];
 #pragma unroll
-        for (int k = 0; k < 6; k++) a[k] = d[k] >= 0 ? flip(__ldg(A.sol + d[k]), (sb >> k) & 1) : 0.0;
+        for (int k = 0; k < 6; k++) a[k] = d[k] >= 0 ? __ldg(A.sol + d[k]) : 0.0;  // signs in C
         double B[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -158,8 +170,7 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
             flag(A.err);
             continue;
         }
-        const unsigned si = (sb >> l) & 1u;
-        const double rv = STIFF ? 0.0 : flip(qsum4<Q4>(nu * b[l], A.qp, w0, adet), si);
+        const double rv = STIFF ? 0.0 : qsum4<Q4>(nu * b[l], A.qp, w0, adet);  // signed through C
         double dv = 0.0;
         if (CALCJ) {
             // the row's six entries first, then its five off-diagonal updates (the six
@@ -179,12 +190,12 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
 #pragma unroll
                 for (int j = 0; j < 6; j++) v[j] = qsum4<Q4>(nu * dot3(C[l], C[j]) + gl * b[j], A.qp, w0, adet);
             }
-            dv = v[l];  // the diagonal: si ^ si = 0, no flip
+            dv = v[l];
 #pragma unroll
             for (int j = 0; j < 6; j++) {
                 if (j == l) continue;
                 const int k = nzb + (int)((pos[l] >> (5 * j)) & 31u);  // absent column: the diagonal
-                slot[k] = slot[k] + flip(v[j], si ^ ((sb >> j) & 1u));
+                slot[k] = slot[k] + v[j];
             }
         }
         if (is < binc) {
