@@ -100,7 +100,11 @@ enum TileMode { kJacobian = 0, kStiffness = 1, kSeeded = 2 };
 //   kSeeded: residual at B, tangent at the seeded state beta B:
 //            nu(|beta B|^2) Ci.Cj + 2 nu'(|beta B|^2) (beta B.Ci)(beta B.Cj), the operation order of
 //            the two-pass seeded kernel.
-template <bool CALCJ, bool Q4, int MODE>
+// FIRST: the block's first colour class. Its slots are all still +0 (no element of the
+// class shares one), so an entry is stored rather than added: slot = v instead of
+// slot = 0 + v, the same value up to the sign of an exact zero, which the store phase
+// normalises (x + 0 turns -0 into +0 and leaves every other value unchanged).
+template <bool CALCJ, bool Q4, int MODE, bool FIRST = false>
 __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, double *__restrict__ slot,
                                              double2 *__restrict__ incv, int bnnz, int binc) {
     const int64_t n = A.nrec;
@@ -195,7 +199,8 @@ __device__ __forceinline__ void tile_element(const TileArgs &A, int64_t i, doubl
             for (int j = 0; j < 6; j++) {
                 if (j == l) continue;
                 const int k = nzb + (int)((pos[l] >> (5 * j)) & 31u);  // absent column: the diagonal
-                slot[k] = slot[k] + v[j];
+                if (FIRST) slot[k] = v[j];
+                else slot[k] = slot[k] + v[j];
             }
         }
         if (is < binc) {
@@ -268,8 +273,12 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int 
             int c0 = 0;
             for (int c = 0; c < ncolors; c++) {
                 const int c1 = Bp->col_end[c];
-                for (int i = c0 + tid; i < c1; i += BT)
-                    tile_element<CALCJ, Q4, MODE>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
+                if (c == 0)
+                    for (int i = c0 + tid; i < c1; i += BT)
+                        tile_element<CALCJ, Q4, MODE, true>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
+                else
+                    for (int i = c0 + tid; i < c1; i += BT)
+                        tile_element<CALCJ, Q4, MODE>(A, (int64_t)rec0 + i, slot, incv, nnz, ninc);
                 c0 = c1;
                 if (c + 1 == ncolors) cp_async_wait_all();
                 __syncthreads();
@@ -317,7 +326,7 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int 
                     if (lane == 0) flag(A.err);
                     continue;
                 }
-                for (int i = lane; i < len; i += 32) A.vals[g + i] = slot[sb0 + i];
+                for (int i = lane; i < len; i += 32) A.vals[g + i] = slot[sb0 + i] + 0.0;  // -0 -> +0
             }
         }
     }
@@ -463,7 +472,8 @@ __global__ void __launch_bounds__(BT, MINB)
         const int c1 = Bp->col_end[c];
         for (int i = c0 + tid; i < c1; i += BT) {
             const int64_t r = (int64_t)rec0 + i;
-            tile_element<true, Q4, kStiffness>(A, r, slot, incv, nnz, ninc);
+            if (c == 0) tile_element<true, Q4, kStiffness, true>(A, r, slot, incv, nnz, ninc);
+            else tile_element<true, Q4, kStiffness>(A, r, slot, incv, nnz, ninc);
             if (!conducting) {
                 const double sg = I.sigma ? __ldg(I.sigma + __ldg(A.recs + 2 * A.nrec + r).z) : 1.0;
                 conducting = fabs(sg) > 1e-12;
@@ -494,10 +504,10 @@ __global__ void __launch_bounds__(BT, MINB)
             if (lane == 0) flag(A.err);
             continue;
         }
-        if (any_m)
-            for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i)] = slot[sb0 + i];
+        if (any_m)  // (+ 0.0: -0 -> +0, the first colour stores its entries)
+            for (int i = lane; i < len; i += 32) I.cvals[2 * (g + i)] = slot[sb0 + i] + 0.0;
         else
-            for (int i = lane; i < len; i += 32) cv2[g + i] = make_double2(slot[sb0 + i], I.omega * 0.0);
+            for (int i = lane; i < len; i += 32) cv2[g + i] = make_double2(slot[sb0 + i] + 0.0, I.omega * 0.0);
     }
     if (!any_m) return;
     // M pass over the same slots
