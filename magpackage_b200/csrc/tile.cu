@@ -268,7 +268,8 @@ __global__ void __launch_bounds__(BT, MINB) k_tile(TileArgs A, int nblocks, int 
             for (int i = tid; i < nchunks; i += BT) cp_async8(schunks + i, A.chunks + chunk0 + i);
         cp_async_commit();
         if (CALCJ) {
-            for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
+            for (int i = tid; i < (nnz + 1) / 2; i += BT)  // 16-byte stores; an odd tail's pair ends in the pad
+        reinterpret_cast<double2 *>(slot)[i] = make_double2(0.0, 0.0);
             __syncthreads();
             int c0 = 0;
             for (int c = 0; c < ncolors; c++) {
@@ -461,7 +462,8 @@ __global__ void __launch_bounds__(BT, MINB)
     for (int i = tid; i < nchunks; i += BT) cp_async8(schunks + i, A.chunks + chunk0 + i);
     cp_async_commit();
     for (int i = tid; i < 18 * nq; i += BT) sval[i] = __ldg(I.val_ref + i);
-    for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
+    for (int i = tid; i < (nnz + 1) / 2; i += BT)  // 16-byte stores; an odd tail's pair ends in the pad
+        reinterpret_cast<double2 *>(slot)[i] = make_double2(0.0, 0.0);
     __syncthreads();
     // K pass; the barrier after its last colour also tells every thread whether any element
     // of the block conducts
@@ -512,7 +514,8 @@ __global__ void __launch_bounds__(BT, MINB)
     if (!any_m) return;
     // M pass over the same slots
     __syncthreads();  // the real parts are read out of the slots
-    for (int i = tid; i < nnz; i += BT) slot[i] = 0.0;
+    for (int i = tid; i < (nnz + 1) / 2; i += BT)  // 16-byte stores; an odd tail's pair ends in the pad
+        reinterpret_cast<double2 *>(slot)[i] = make_double2(0.0, 0.0);
     __syncthreads();
     c0 = 0;
     for (int c = 0; c < ncolors; c++) {
