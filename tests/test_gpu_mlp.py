@@ -31,6 +31,39 @@ def test_forward_matches_oracle(n):
     assert np.corrcoef(y, y_ref)[0, 1] > 0.99999
 
 
+@pytest.mark.parametrize("use_rows", [True, False])
+def test_predict_nu_scatter_and_clamp(use_rows):
+    """mag_mlp_predict_nu: nu = clamp(exp(y * scale + shift), nu_min, nu_max), scattered to
+    d_nu[d_rows[i]] (d_rows NULL: d_nu[i]); y is the inference output of the same network,
+    checked against the oracle like the forward test. Rows not named keep their values."""
+    n = 5000
+    p, x, _ = _case(n, 4)
+    net = MLP(p)
+    xd = torch.as_tensor(x, device="cuda")
+    y, _ = net.forward(xd)
+    y = y.cpu().numpy().astype(np.float64)
+    scale, shift = 0.7, 3.0
+    lo = float(np.exp(np.quantile(y, 0.1) * scale + shift))
+    hi = float(np.exp(np.quantile(y, 0.9) * scale + shift))
+    m = n + 17  # the output is longer than the rows: the extra entries are not touched
+    perm = np.random.default_rng(5).permutation(m)[:n].astype(np.int32)
+    rows = torch.as_tensor(perm, device="cuda") if use_rows else None
+    nu = torch.full((m,), -1.0, dtype=torch.float64, device="cuda")
+    net.predict_nu(xd, rows, nu, scale, shift, lo, hi)
+    net.check()
+    got = nu.cpu().numpy()
+    idx = perm if use_rows else np.arange(n)
+    want = np.clip(np.exp(y * scale + shift), lo, hi)
+    np.testing.assert_allclose(got[idx], want, rtol=1e-13, atol=0)
+    assert np.sum(want == lo) > 0 and np.sum(want == hi) > 0  # both bounds were hit
+    untouched = np.ones(m, dtype=bool)
+    untouched[idx] = False
+    assert np.all(got[untouched] == -1.0)
+    y_ref, _ = mlp_ref.forward(p, x)
+    want_ref = np.clip(y_ref * scale + shift, np.log(lo), np.log(hi))
+    assert np.max(np.abs(np.log(got[idx]) - want_ref)) <= scale * 2e-3 * (1 + np.max(np.abs(y_ref)))
+
+
 @pytest.mark.parametrize("n", [256, 1000])
 def test_gradient_matches_oracle(n):
     p, x, t = _case(n, 2)
