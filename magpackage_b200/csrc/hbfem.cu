@@ -37,16 +37,26 @@ struct HbArgs {
 // Index of (r, c), r <= c, in the upper triangle of a 6 x 6 block stored row by row.
 __host__ __device__ constexpr int kb_at(int r, int c) { return r * 6 - r * (r - 1) / 2 + (c - r); }
 
-// Resident CTAs per SM the element kernel is compiled for (registers <= 65536 / (128 x this)).
+// Resident CTAs per SM the element kernel is compiled for (registers <= 65536 / (128 x this)):
+// with the harmonic count a compile-time constant (MAG_HBFEM_MINB) and at run time
+// (MAG_HBFEM_MINB_RT). Measured at 40^3, K = 3, N = 32: run-time count 3.26 ms (3 CTAs/SM);
+// constant count 2.24 ms (3 CTAs/SM, 168 registers) and 1.66 ms (2 CTAs/SM, 255 registers).
 #ifndef MAG_HBFEM_MINB
-#define MAG_HBFEM_MINB 3
+#define MAG_HBFEM_MINB 2
+#endif
+#ifndef MAG_HBFEM_MINB_RT
+#define MAG_HBFEM_MINB_RT 3
 #endif
 
-template <bool CALCJ>
-__global__ void __launch_bounds__(128, MAG_HBFEM_MINB) k_hbfem_elems(HbArgs A) {
+// KC: the harmonic count as a compile-time constant (0: A.K at run time, arrays sized for
+// kMaxHarm); with a constant count the harmonic loops unroll and the arrays are indexed
+// statically.
+template <bool CALCJ, int KC>
+__global__ void __launch_bounds__(128, KC > 0 ? MAG_HBFEM_MINB : MAG_HBFEM_MINB_RT) k_hbfem_elems(HbArgs A) {
+    constexpr int KA = KC > 0 ? KC : kMaxHarm;
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= A.m.ne) return;
-    const int K = A.K, N = A.N;
+    const int K = KC > 0 ? KC : A.K, N = A.N;
     const int4 tt = A.m.tet[e];
     int d[6];
     load_dofs(A.m.dofs, e, d);
@@ -54,7 +64,7 @@ __global__ void __launch_bounds__(128, MAG_HBFEM_MINB) k_hbfem_elems(HbArgs A) {
     const int tag = A.m.tags[e];
     Geo g;
     geometry(A.m.xyz, tt, g);
-    double ar[6][kMaxHarm], ai[6][kMaxHarm];
+    double ar[6][KA], ai[6][KA];
     for (int k = 0; k < 6; k++)
         for (int h = 0; h < K; h++) {
             const bool has = d[k] >= 0;
@@ -63,7 +73,7 @@ __global__ void __launch_bounds__(128, MAG_HBFEM_MINB) k_hbfem_elems(HbArgs A) {
             ar[k][h] = flip(xr, (sb >> k) & 1);
             ai[k][h] = flip(xi, (sb >> k) & 1);
         }
-    double rr[6][kMaxHarm], ri[6][kMaxHarm];
+    double rr[6][KA], ri[6][KA];
     for (int k = 0; k < 6; k++)
         for (int h = 0; h < K; h++) {
             rr[k][h] = 0.0;
@@ -167,8 +177,13 @@ int launch_hbfem(const ElemData &m, const RowPlan &rp, int max_row, const double
                  double *out_re, double *out_im, cudaStream_t s) {
     HbArgs A{m, sr, si, dr, di, pr, pi, K, N, rp.ndof, qp, mp, vals ? scratch : nullptr, rscr};
     const unsigned g = (unsigned)((m.ne + 127) / 128);
-    if (vals) k_hbfem_elems<true><<<g, 128, 0, s>>>(A);
-    else k_hbfem_elems<false><<<g, 128, 0, s>>>(A);
+    switch (K) {
+        case 1: vals ? k_hbfem_elems<true, 1><<<g, 128, 0, s>>>(A) : k_hbfem_elems<false, 1><<<g, 128, 0, s>>>(A); break;
+        case 2: vals ? k_hbfem_elems<true, 2><<<g, 128, 0, s>>>(A) : k_hbfem_elems<false, 2><<<g, 128, 0, s>>>(A); break;
+        case 3: vals ? k_hbfem_elems<true, 3><<<g, 128, 0, s>>>(A) : k_hbfem_elems<false, 3><<<g, 128, 0, s>>>(A); break;
+        case 4: vals ? k_hbfem_elems<true, 4><<<g, 128, 0, s>>>(A) : k_hbfem_elems<false, 4><<<g, 128, 0, s>>>(A); break;
+        default: vals ? k_hbfem_elems<true, 0><<<g, 128, 0, s>>>(A) : k_hbfem_elems<false, 0><<<g, 128, 0, s>>>(A);
+    }
     if (cudaPeekAtLastError() != cudaSuccess) return MAG_E_CUDA;
     const int64_t nt = rp.ndof * 2 * K;
     k_rows_reduce_harm<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(rp, rscr, K, out_re, out_im);

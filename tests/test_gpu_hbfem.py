@@ -30,7 +30,8 @@ def _case(port, harmonics, n=(5, 4, 3), seed=12, scale=1.0, imag=True):
     return plan, m, pk, sol, E
 
 
-@pytest.mark.parametrize("harmonics,imag", [((0, 1, 3), True), ((1, 3, 5, 7), True), ((0, 1), False)])
+@pytest.mark.parametrize("harmonics,imag", [((0, 1, 3), True), ((1, 3, 5, 7), True), ((0, 1), False), ((1,), True),
+                                            ((1, 3, 5, 7, 9), True)])
 def test_hbfem_matches_oracle(oracle_port, harmonics, imag):
     plan, m, pk, sol, E = _case(oracle_port, harmonics, imag=imag)
     aft = AFT(harmonics)
