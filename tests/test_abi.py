@@ -59,3 +59,16 @@ def test_mex_entry_points_accept_an_empty_mesh():
     assert L.mag_mex_jacobian(*args_j) == 0
     assert L.mag_mex_curl_curl(p, 1, p, 0, p, p, p, p, 4, p, p, p, p) == 0
     assert L.mag_mex_mass(p, 1, p, 0, p, p, None, 0, p, 4, p, p, p, p) == 0
+
+
+def test_product_path_fails_loudly_without_its_library_or_a_gpu(monkeypatch):
+    """No CPU fallback: a missing library and a machine without a CUDA device are errors."""
+    import pytest
+    import torch
+
+    monkeypatch.setattr(_lib, "_LIB", None)
+    with pytest.raises(FileNotFoundError):
+        _lib.load(os.path.join(ROOT, "no_such_dir", "libmagasm.so"))
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
+    with pytest.raises(RuntimeError, match="no CPU path"):
+        _lib.lib()
