@@ -94,6 +94,14 @@ typedef struct {
 
 int mag_version(void);
 const char *mag_last_error(void);
+/* Threading. Every handle-based entry point only enqueues work on its stream and
+ * returns; mag_sync waits for the stream (MAG_E_CUDA with the CUDA error text if
+ * work on it failed). Different handles may be used from different host threads at
+ * once; one handle is used by one thread at a time. The MEX entry points run one at
+ * a time (they share the mesh cache and the staging buffers) and return with their
+ * outputs on the host, as the reference's gateways do (they are single-threaded
+ * callees of MATLAB: assemble_jacobian_kernel_mex.cpp:8-153). */
+int mag_sync(void *stream);
 
 /* ---- topology ------------------------------------------------------------ */
 

@@ -42,6 +42,7 @@ _int = C.c_int
 _PROTOS = {
     "mag_version": ([], _int),
     "mag_last_error": ([], C.c_char_p),
+    "mag_sync": ([_vp], _int),
     "mag_generate_edges": ([_vp, _i64, _i64, _vp, _vp, _vp, C.POINTER(_i64), _vp], _int),
     "mag_mesh_create": ([_vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, C.POINTER(_vp), _vp], _int),
     "mag_mesh_destroy": ([_vp], _int),
@@ -157,6 +158,11 @@ def dptr(a):
     if a is None:
         return None
     return a.ctypes.data_as(_dp)
+
+
+def sync(stream=None) -> None:
+    """mag_sync: wait for the stream's enqueued work; raises MagError if it failed."""
+    check(lib().mag_sync(stream_ptr(stream)))
 
 
 def stream_ptr(stream=None):

@@ -407,6 +407,15 @@ extern "C" {
 int mag_version(void) { return 1; }
 const char *mag_last_error(void) { return g_err; }
 
+int mag_sync(void *stream) {
+    const cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) {
+        set_error("mag_sync: %s", cudaGetErrorString(e));
+        return MAG_E_CUDA;
+    }
+    return MAG_OK;
+}
+
 int mag_generate_edges(const int32_t *d_T, int64_t Ne, int64_t Nn, int32_t *d_edges, int32_t *d_t2e,
                        int8_t *d_sign, int64_t *E_out, void *stream) {
     return generate_edges(d_T, Ne, Nn, d_edges, d_t2e, d_sign, E_out, (cudaStream_t)stream);

@@ -270,6 +270,35 @@ def test_explicit_signs_are_honoured(oracle_port):
     assert bits_equal(host(res), oracle_port.sparse_vec(Ri, Rv, E))
 
 
+def test_async_calls_on_side_streams_and_mag_sync(oracle_port):
+    """The handle API only enqueues: two handles assembling on two streams, each waited for
+    with mag_sync, give the same bits as a call on the current stream."""
+    mesh = synth.kuhn_box(5, seed=4)
+    tags = synth.cube_layout(mesh)
+    packed = material.pack_material_data(synth.standard_materials())
+    edges, t2e, sign = oracle_port.generate_edges(mesh.T)
+    E = edges.shape[0]
+    sol = torch.as_tensor(np.random.default_rng(9).normal(0, 0.05, E), device="cuda")
+    plans = [AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign) for _ in range(2)]
+    for p in plans:
+        p.set_materials(packed)
+    v0, r0 = plans[0].jacobian(sol)
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    out = []
+    for p, s in zip(plans, streams):
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            vals, res = p.new_values(), p.new_vector()
+        p.jacobian(sol, vals, res, stream=s)
+        out.append((vals, res, s))
+    for vals, res, s in out:
+        _lib.sync(s)
+        assert torch.equal(vals, v0) and torch.equal(res, r0)
+    for p in plans:
+        p.close()
+
+
 def test_deterministic_repeat(oracle_port):
     mesh, tags, edges, t2e, sign, m, E, sol = _nonlinear_case(oracle_port, 10, 4)
     plan = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
