@@ -13,7 +13,8 @@
 //
 // Rounding points (mirrored by oracle/mlp_ref.py): layer inputs are rounded to
 // BF16 before each MMA; accumulation, biases, activations, the last (64 -> 1)
-// layer and all gradients are FP32.
+// layer and all gradients are FP32. Inference halves W1..W3 and b1..b3 (exact),
+// so that its accumulators hold z/2 and SiLU takes one FMA after the tanh.
 #include <cuda_bf16.h>
 
 #include <cstdint>
@@ -199,35 +200,32 @@ __device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
     asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
     return r;
 }
-__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
-    uint64_t r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
 __device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
     uint64_t r;
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
     return r;
 }
 
-// SiLU of a hidden pair (z0, z1), packed as BF16 (z0 in the low half): z * (1/2 + tanh(z/2)/2),
-// one single-precision tanh.approx per value, the arithmetic around it on packed pairs.
+// SiLU of a hidden pair from its halved pre-activations h = z/2, packed as BF16 (z0's
+// value in the low half). The inference kernel halves W1..W3 and b1..b3 (exact: a power of
+// two), so the accumulators hold h, and z sigmoid(z) = h (1 + tanh h) = h + h tanh h: one
+// single-precision tanh.approx per value and one packed FMA per pair.
 // (A half-precision tanh of the pair, one MUFU operation for two values, was measured: 4 %
 // faster at 8M rows, but its forward error, 6.7e-3 of max|y|, is above the 5.6e-3 bound.)
-__device__ __forceinline__ uint32_t silu2_bf16(uint64_t z) {
-    const uint64_t half2 = pk2(0.5f, 0.5f);
+__device__ __forceinline__ uint32_t silu2h_bf16(uint64_t h) {
     float h0, h1, t0, t1;
-    upk2(mul2(z, half2), h0, h1);
+    upk2(h, h0, h1);
     asm("tanh.approx.f32 %0, %1;" : "=f"(t0) : "f"(h0));
     asm("tanh.approx.f32 %0, %1;" : "=f"(t1) : "f"(h1));
     float p0, p1;
-    upk2(mul2(z, fma2(pk2(t0, t1), half2, half2)), p0, p1);
+    upk2(fma2(h, pk2(t0, t1), h), p0, p1);
     uint32_t out;
     asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(out) : "f"(p1), "f"(p0));
     return out;
 }
 
-// Inference form of hidden_epilogue: the same image, packed arithmetic.
+// Inference form of hidden_epilogue: the same image, packed arithmetic on the halved
+// accumulators and biases (h = z/2).
 __device__ __forceinline__ void hidden_epilogue_infer(uint32_t tmem, const float *bias, __nv_bfloat16 *img,
                                                       int row_t) {
 #pragma unroll
@@ -238,8 +236,8 @@ __device__ __forceinline__ void hidden_epilogue_infer(uint32_t tmem, const float
 #pragma unroll
         for (int i = 0; i < 8; i += 2) {  // one 16-byte shared load of biases per two pairs
             const float4 b = *reinterpret_cast<const float4 *>(bias + c + 2 * i);
-            hp[i] = silu2_bf16(add2(pk2(z[2 * i], z[2 * i + 1]), pk2(b.x, b.y)));
-            hp[i + 1] = silu2_bf16(add2(pk2(z[2 * i + 2], z[2 * i + 3]), pk2(b.z, b.w)));
+            hp[i] = silu2h_bf16(add2(pk2(z[2 * i], z[2 * i + 1]), pk2(b.x, b.y)));
+            hp[i + 1] = silu2h_bf16(add2(pk2(z[2 * i + 2], z[2 * i + 3]), pk2(b.z, b.w)));
         }
         *reinterpret_cast<uint4 *>(img + core_off(row_t, c, kH)) = *reinterpret_cast<uint4 *>(hp);
         *reinterpret_cast<uint4 *>(img + core_off(row_t, c + 8, kH)) = *reinterpret_cast<uint4 *>(hp + 4);
@@ -270,6 +268,21 @@ __device__ __forceinline__ void load_ops(Smem &S, const __nv_bfloat16 *ops, int 
     const uint4 *src = reinterpret_cast<const uint4 *>(ops + first);
     uint4 *dst = reinterpret_cast<uint4 *>(S.w);
     for (int i = threadIdx.x; i < count / 8; i += blockDim.x) dst[i] = src[i];
+}
+
+// load_ops with every weight halved (a power-of-two scale: exact for every weight above
+// 2^-125 in magnitude, where BF16 values are normal).
+__device__ __forceinline__ void load_ops_halved(Smem &S, const __nv_bfloat16 *ops, int first, int count) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(ops + first);
+    uint4 *dst = reinterpret_cast<uint4 *>(S.w);
+    const __nv_bfloat162 half2 = __floats2bfloat162_rn(0.5f, 0.5f);
+    for (int i = threadIdx.x; i < count / 8; i += blockDim.x) {
+        uint4 v = src[i];
+        __nv_bfloat162 *p = reinterpret_cast<__nv_bfloat162 *>(&v);
+#pragma unroll
+        for (int j = 0; j < 4; j++) p[j] = __hmul2(p[j], half2);
+        dst[i] = v;
+    }
 }
 
 __device__ __forceinline__ void tmem_alloc(Smem &S) {
@@ -348,12 +361,15 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
         mbar_init(&S.bar);
         S.fail = 0;
     }
-    // all weight images: W1p | W2 | W3 (contiguous in the operand buffer)
-    load_ops(S, a.ops, bW1p, kW1pElems + 2 * kWElems);
+    // all weight images: W1p | W2 | W3 (contiguous in the operand buffer). Inference halves
+    // W1..W3 and b1..b3 (exact), so that the accumulators hold z/2 (silu2h_bf16).
+    const float hs = INFER ? 0.5f : 1.0f;
+    if (INFER) load_ops_halved(S, a.ops, bW1p, kW1pElems + 2 * kWElems);
+    else load_ops(S, a.ops, bW1p, kW1pElems + 2 * kWElems);
     for (int i = t; i < kH; i += kRows) {
-        S.vec[i] = a.params[ob1 + i];
-        S.vec[kH + i] = a.params[ob2 + i];
-        S.vec[2 * kH + i] = a.params[ob3 + i];
+        S.vec[i] = hs * a.params[ob1 + i];
+        S.vec[kH + i] = hs * a.params[ob2 + i];
+        S.vec[2 * kH + i] = hs * a.params[ob3 + i];
         S.vec[3 * kH + i] = a.params[ow4 + i];
     }
     if (t == 0) S.vec[4 * kH] = a.params[ob4];
@@ -417,8 +433,7 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
         // layer 3 and the 64 -> 1 output, 16 columns at a time
         if (!run_layer_fwd(S, W3, kH, phase, a.spin_limit, ok)) break;
         float y = 0.0f;
-        if (INFER) {  // pairs: single-precision tanh (the output is not rounded to BF16)
-            const uint64_t half2 = pk2(0.5f, 0.5f);
+        if (INFER) {  // pairs of halved pre-activations: single-precision tanh (the output is not rounded to BF16)
             uint64_t yacc = pk2(0.0f, 0.0f);
 #pragma unroll
             for (int c = 0; c < kH; c += 16) {
@@ -434,13 +449,12 @@ __global__ void __launch_bounds__(kRows, 6) k_mlp_forward(MlpForwardArgs a) {
                     }
                     const float2 b = (i & 1) ? make_float2(b4.z, b4.w) : make_float2(b4.x, b4.y);
                     const float2 w = (i & 1) ? make_float2(w4.z, w4.w) : make_float2(w4.x, w4.y);
-                    const uint64_t zz = add2(pk2(z[2 * i], z[2 * i + 1]), pk2(b.x, b.y));
+                    const uint64_t hh = add2(pk2(z[2 * i], z[2 * i + 1]), pk2(b.x, b.y));  // z/2
                     float h0, h1, t0, t1;
-                    upk2(mul2(zz, half2), h0, h1);
+                    upk2(hh, h0, h1);
                     asm("tanh.approx.f32 %0, %1;" : "=f"(t0) : "f"(h0));
                     asm("tanh.approx.f32 %0, %1;" : "=f"(t1) : "f"(h1));
-                    const uint64_t sg = fma2(pk2(t0, t1), half2, half2);
-                    yacc = fma2(pk2(w.x, w.y), mul2(zz, sg), yacc);
+                    yacc = fma2(pk2(w.x, w.y), fma2(hh, pk2(t0, t1), hh), yacc);  // w4 silu(z)
                 }
             }
             float y0, y1;
