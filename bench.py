@@ -16,7 +16,7 @@ inference over every element. ``--workload jacobian_60`` is the 60^3 case.
   cpu_baseline -- the reference's own C++/OpenMP MEX kernel (compiled
             unchanged into oracle/_ref) plus the restated MATLAB sparse(),
             on the host cores, one full assembly; its CSR and residual are
-            then the checker of the GPU's output ("parity").
+            then the reference the GPU output is compared with ("parity").
 
 ``--impl reference`` times that CPU path alone as the reference arm.
 Multi-GPU (torchrun): every rank assembles its own instance of the workload
@@ -740,7 +740,7 @@ def main():
                "sample": f"one full {args.workload} assembly ({ne} tets): MEX kernel {k * 1e3:.0f} ms "
                          f"+ sparse() {s * 1e3:.0f} ms, OpenMP on all host threads"}
         parity = parity_against(ref, plan, vals, res)
-        parity["checker"] = f"{kind} MEX kernel + restated sparse(), same mesh and state"
+        parity["compared_with"] = f"{kind} MEX kernel + restated sparse(), same mesh and state"
         del ref
 
     if rank == 0:

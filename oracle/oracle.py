@@ -8,7 +8,7 @@ Two CPU implementations of the reference's element-assembly path:
   restates Mesh.generateEdges, MATLAB sparse() and pchip.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
-module, and only as the checker or the timed CPU baseline; the product path
+module, and only as the reference results to compare with or the timed CPU baseline; the product path
 never imports it. Inputs follow the reference's MEX boundary (Assembler.m):
 column-major doubles with 1-based indices.
 """

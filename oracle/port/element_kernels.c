@@ -1,6 +1,6 @@
 /*
  * CPU restatement of the reference's four Nedelec element kernels.
- * TEST INFRASTRUCTURE ONLY (the checker; see oracle.h).
+ * TEST INFRASTRUCTURE ONLY (results to compare the GPU with; see oracle.h).
  *
  * The floating-point operations are evaluated in the same order as the
  * reference MEX sources so that this restatement is bit-identical to them

@@ -1,7 +1,7 @@
 /*
  * CPU restatement of MagPackage's Nedelec element-assembly path.
  *
- * TEST INFRASTRUCTURE ONLY: this library is the checker for the CUDA path.
+ * TEST INFRASTRUCTURE ONLY: the CUDA path is compared with this library.
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
  * it. Parity is pinned: tests/test_oracle.py checks every function here against
  * the reference's own MEX kernels compiled unchanged (oracle/_ref) and against

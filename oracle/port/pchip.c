@@ -1,6 +1,6 @@
 /*
  * CPU restatement of MATLAB's pchip(x, y), the B-H table builder that
- * src/MaterialLib.m:117 calls. TEST INFRASTRUCTURE ONLY (the checker).
+ * src/MaterialLib.m:117 calls. TEST INFRASTRUCTURE ONLY (results to compare the GPU with).
  *
  * MATLAB is not installed, so this follows MATLAB's published algorithm
  * (Fritsch-Carlson monotone slopes: interior slope = scaled weighted harmonic

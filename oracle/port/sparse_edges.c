@@ -1,6 +1,6 @@
 /*
  * CPU restatement of the MATLAB-side steps around the element kernels.
- * TEST INFRASTRUCTURE ONLY (the checker; see oracle.h).
+ * TEST INFRASTRUCTURE ONLY (results to compare the GPU with; see oracle.h).
  *   oracle_generate_edges  src/Mesh.m:114-138
  *   oracle_sparse_csr      MATLAB sparse() as called at src/Assembler.m:37-38, 205-206
  *   oracle_sparse_vec      src/Assembler.m:211-216

@@ -7,7 +7,7 @@ their largest) Froehlich Jacobians, the 64-mesh complex frequency batch, and the
 transient box (40x40x20, 192k tets) after one Newton-converged step. Each compares the
 CSR pattern bit for bit and reports the per-nonzero maximum relative error and the
 Frobenius relative error against the oracle (the restated MATLAB sparse() of the
-reference MEX triplets); the bound is bit equality (north star: 1e-12 per nonzero).
+reference MEX triplets); the bound is bit equality (the required bound is 1e-12 relative per nonzero).
 """
 import json
 

@@ -4,7 +4,7 @@ Every CSR produced on the GPU is compared with the oracle's restatement of
 MATLAB's sparse() applied to the reference MEX triplets (the compiled
 reference when oracle/_ref is present, its pinned C restatement otherwise):
 row_ptr/col_idx must be identical and every value identical bit for bit
-(tolerance 0; the north-star bound is 1e-12 relative per nonzero).
+(tolerance 0; the required bound is 1e-12 relative per nonzero).
 """
 import ctypes as C
 
@@ -20,7 +20,7 @@ from oracle.oracle import mex_inputs
 
 pytestmark = pytest.mark.gpu
 
-REL_TOL = 1e-12  # north-star bound per nonzero; the tests below demand exact equality
+REL_TOL = 1e-12  # required bound per nonzero; the tests below demand exact equality
 
 
 def dev(a, dtype=torch.float64):
