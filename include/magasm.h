@@ -458,8 +458,10 @@ int mag_sparse_destroy(mag_sparse *sp);
  * material tables are host arrays, as in mag_mex_jacobian. The element blocks
  * go to a static device array inside the library (Ne <= 32768, nmat <= 64,
  * nbrk <= 4096, ncoe <= 16384; larger sizes return MAG_E_UNSUPPORTED), which
- * every GPU that loads the library holds until exit. No call can be captured
- * into a CUDA graph: each copies the host tables and synchronises `stream`.
+ * every GPU that loads the library holds until exit. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress, once per
+ * device): make it before any stream capture begins. Each call copies the host
+ * tables and synchronises `stream`.
  * With lazy module loading (CUDA's default) the first call on a device is when the
  * array is committed on the device, and it can fail with MAG_E_CUDA when the
  * device has no memory left, so make it early. Calls share the array: calls

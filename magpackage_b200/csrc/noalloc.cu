@@ -18,9 +18,9 @@
 // streams, or different host threads) race on the array: serialise them.
 //
 // The first call on each device looks up the array's device address with
-// cudaGetSymbolAddress (with that device current) and caches it. No call can be
-// captured into a CUDA graph: each copies the host tables from pageable memory and
-// synchronises the stream. With CUDA's lazy module loading
+// cudaGetSymbolAddress (with that device current) and caches it; make that first
+// call before any stream capture begins. Each call copies the host tables from
+// pageable memory and synchronises the stream. With CUDA's lazy module loading
 // (the default) the array is committed on a device at that first call, not when
 // the library is loaded, so a first call made under a tight memory budget can
 // fail for lack of device memory (MAG_E_CUDA); make it early. Nothing here calls
