@@ -295,16 +295,36 @@ def run_transient(args):
 
 
 def run_batched_complex(args):
-    """Config 3: 64 uneven meshes, complex K + j*omega*sigma*M, one graph-captured launch."""
+    """Config 3: 64 uneven meshes, complex K + j*omega*sigma*M, one graph-captured launch.
+
+    Under torchrun the meshes are split across the ranks by partition_instances (largest
+    first, to the least-loaded rank; no exchange): each rank assembles its share in one
+    batch and value = all meshes' elements / the slowest rank's time (strong scaling: the
+    64 meshes are the whole job at every N)."""
     import torch
 
     from magpackage_b200 import synth
+    from magpackage_b200.partition import partition_instances
     from magpackage_b200.plan import AssemblyPlan, ComplexBatch, generate_edges
 
-    torch.cuda.set_device(0)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    sizes = synth.frequency_sweep_sizes(count=args.instances)
+    mine = set(partition_instances(sizes, world)[rank])
     plans, nus, sigmas, omegas = [], [], [], []
     ne_total = nnz_total = nodes_total = edges_total = 0
-    for mesh, tags, nu, sigma, omega in synth.frequency_sweep_instances(count=args.instances, seed=0):
+    for k, (mesh, tags, nu, sigma, omega) in enumerate(
+            synth.frequency_sweep_instances(count=args.instances, seed=0)):
+        if k not in mine:  # (every rank draws every instance: their layouts share one stream)
+            continue
         edges, t2e, sign = generate_edges(mesh.T)
         E = int(edges.shape[0])
         p = AssemblyPlan(mesh.P, mesh.T, t2e, E, tags, sign)
@@ -316,33 +336,48 @@ def run_batched_complex(args):
         nnz_total += p.nnz
         nodes_total += mesh.num_nodes
         edges_total += E
-    batch = ComplexBatch(plans, nus, sigmas, omegas)
-    chosen, times, name = batch.tuning()
+    batch = ComplexBatch(plans, nus, sigmas, omegas) if plans else None
+    chosen, times, name = batch.tuning() if batch else (None, [], "none (no mesh on this rank)")
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
-        batch.assemble()
+        if batch:
+            batch.assemble()
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        batch.assemble()
+        if batch:
+            batch.assemble()
     ev1.record(stream)
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    b_alg = (41.0 * ne_total + 24.0 * nodes_total + 16.0 * nnz_total + 8.0 * ne_total * 2)
+    if dist is not None:
+        dist.barrier()
+    ms_mine = ev0.elapsed_time(ev1) / args.steps
+    b_alg_mine = (41.0 * ne_total + 24.0 * nodes_total + 16.0 * nnz_total + 8.0 * ne_total * 2)
+    ms, b_alg, ne_all, nnz_all = max_over_ranks([ms_mine], dist, "cuda")[0], b_alg_mine, ne_total, nnz_total
+    if dist is not None:  # the job's totals (after the timed region)
+        tot = torch.tensor([b_alg_mine, float(ne_total), float(nnz_total)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tot)
+        b_alg, ne_all, nnz_all = float(tot[0]), int(tot[1]), int(tot[2])
     peak, kind = measured_peak()
-    out = {"metric": "batched complex assembly Melem/s (complex128 CSR)", "value": ne_total / ms / 1e3,
-           "unit": "Melem/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-           "higher_is_better": True, "dtype": "f64->c128", "data": "synthetic",
-           "config": {"workload": f"{args.instances} jittered cubes 8^3..48^3 hexes x6, K + j*omega*sigma*M, "
-                                  "10 Hz-10 kHz",
-                      "elements": ne_total, "nnz": nnz_total, "variant": name,
-                      "variant_times_ms": [round(float(t), 4) for t in times]},
-           "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                        "frac": b_alg / (ms * 1e-3) / 1e9 / peak, "peak_source": kind,
-                        "bytes_per_elem": b_alg / ne_total},
-           "gpu_launches": args.steps}
-    print(json.dumps(out), flush=True)
+    if rank == 0:
+        out = {"metric": "batched complex assembly Melem/s (complex128 CSR)", "value": ne_all / ms / 1e3,
+               "unit": "Melem/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+               "higher_is_better": True, "scaling": "strong", "dtype": "f64->c128", "data": "synthetic",
+               "config": {"workload": f"{args.instances} jittered cubes 8^3..48^3 hexes x6, K + j*omega*sigma*M, "
+                                      "10 Hz-10 kHz",
+                          "elements": ne_all, "nnz": nnz_all, "variant": name,
+                          "variant_times_ms": [round(float(t), 4) for t in times],
+                          "parallelism": f"meshes split across {world} rank(s), no exchange"},
+               "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9 / world, "peak": peak,
+                            "unit": "GB/s", "frac": b_alg / (ms * 1e-3) / 1e9 / world / peak,
+                            "peak_source": kind, "bytes_per_elem": b_alg / ne_all, "per": "GPU"},
+               "gpu_launches": args.steps}
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 # Elements per reference-arm step: a full 110^3 CPU assembly takes ~13 s, so each step

@@ -208,6 +208,17 @@ def standard_materials(iron_nonlinear: bool = True):
 SIGMA_AL = 3.526e7
 
 
+def frequency_sweep_sizes(count: int = 64, n_min: int = 8, n_max: int = 48) -> list[int]:
+    """Tetrahedra of each instance of frequency_sweep_instances (6 n_k^3), without building
+    the meshes."""
+    out = []
+    for k in range(count):
+        t = k / max(count - 1, 1)
+        n = int(round(n_min + (n_max - n_min) * t))
+        out.append(6 * n ** 3)
+    return out
+
+
 def frequency_sweep_instances(count: int = 64, n_min: int = 8, n_max: int = 48, f_min: float = 10.0,
                               f_max: float = 1e4, seed: int = 0):
     """Independent jittered cubes of uneven size for the batched complex workload.

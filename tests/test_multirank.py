@@ -64,3 +64,75 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
     args = argparse.Namespace(steps=1, warmup=1)
     bench.run_reference_arm(args, rank=1, world=2, workload="jacobian_60")
     assert capsys.readouterr().out == ""  # a non-zero rank does no work and prints nothing
+
+
+def _partition_rank_main(rank, world, port, out):
+    sys.path.insert(0, ROOT)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+
+    import torch
+
+    from magpackage_b200 import synth
+    from magpackage_b200.partition import partition_instances
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        sizes = synth.frequency_sweep_sizes(64)
+        mine = partition_instances(sizes, world)[rank]  # computed locally: no exchange
+        # what the ranks would assemble, gathered only to check the split
+        t = torch.zeros(64, dtype=torch.int64)
+        t[mine] = rank + 1
+        got = [torch.zeros(64, dtype=torch.int64) for _ in range(world)]
+        dist.all_gather(got, t)
+        out.put((rank, mine, [g.tolist() for g in got]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_frequency_sweep_meshes_split_across_two_gloo_ranks():
+    """Config 3's 64 meshes are independent: each rank computes the same split from the
+    meshes' sizes, with no exchange, and assembles its own part. Gathered here only to
+    check it: every mesh on exactly one rank, loads within the largest mesh of each other."""
+    from magpackage_b200 import synth
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_partition_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    sizes = synth.frequency_sweep_sizes(64)
+    owner = [0] * 64
+    for rank, mine, gathered in res:
+        assert gathered == res[0][2]  # both ranks see the same assignment
+        for i in mine:
+            assert owner[i] == 0
+            owner[i] = rank + 1
+    assert all(o in (1, 2) for o in owner) and owner == [max(g[i] for g in res[0][2]) for i in range(64)]
+    loads = [sum(s for s, o in zip(sizes, owner) if o == r + 1) for r in range(2)]
+    assert abs(loads[0] - loads[1]) <= max(sizes)
+
+
+def test_partition_instances_properties():
+    from magpackage_b200.partition import partition_instances, rank_loads
+
+    rng = __import__("numpy").random.default_rng(3)
+    for world in (1, 2, 3, 4, 8, 70):
+        sizes = [int(x) for x in rng.integers(0, 10_000, size=64)]
+        parts = partition_instances(sizes, world)
+        assert len(parts) == world
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(64))  # a partition of the instances
+        assert all(p == sorted(p) for p in parts)
+        loads = rank_loads(sizes, parts)
+        assert max(loads) - min(loads) <= max(sizes)  # largest-first to the least loaded
+        assert parts == partition_instances(sizes, world)  # deterministic
+    assert partition_instances([], 3) == [[], [], []]
+    with pytest.raises(ValueError):
+        partition_instances([1, 2], 0)
