@@ -230,3 +230,39 @@ def test_element_b_restatement_patch_test(oracle_port):
     phi = np.random.default_rng(3).normal(size=mesh.num_nodes)
     B, scale = element_b(mesh.P, mesh.T, t2e, sign, phi[edges[:, 1]] - phi[edges[:, 0]])
     assert np.all(np.abs(B) <= 1e-12 * scale)
+
+
+def test_mlp_oracle_gradient_matches_finite_differences(monkeypatch):
+    """The MLP oracle's backward pass (oracle/mlp_ref.py), which the GPU gradient kernels
+    are checked against, pinned by central differences of its own loss
+    L = sum_i s/2 (y_i - t_i)^2 with the BF16 rounding switched off (the backward pass
+    treats each rounding as the identity, so without it the two must agree to
+    finite-difference accuracy)."""
+    from magpackage_b200.mlp import init_params
+    from oracle import mlp_ref
+
+    monkeypatch.setattr(mlp_ref, "bf16", lambda x: np.asarray(x, dtype=np.float64))
+    rng = np.random.default_rng(8)
+    p = init_params(2).astype(np.float64)
+    p[256:320] = rng.normal(0, 0.1, 64)
+    x = rng.normal(0, 1, (37, 4))
+    t = rng.normal(0, 1, 37)
+    s = 0.5
+
+    def loss(q):
+        y, _ = mlp_ref.forward(q, x)
+        return float(np.sum(0.5 * s * (y - t) ** 2))
+
+    _, g = mlp_ref.gradient(p, x, t, s)
+    assert g.shape == (mlp_ref.NPARAMS,)
+    # a few parameters of every block: W1, b1, W2, b2, W3, b3, w4, b4
+    starts = [0, 256, 320, 4416, 4480, 8576, 8640, 8704]
+    idx = sorted({int(i) for st, en in zip(starts, starts[1:] + [mlp_ref.NPARAMS])
+                  for i in rng.integers(st, en, size=6)})
+    for i in idx:
+        h = 1e-6 * max(1.0, abs(p[i]))
+        q1, q2 = p.copy(), p.copy()
+        q1[i] += h
+        q2[i] -= h
+        fd = (loss(q1) - loss(q2)) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * (1.0 + abs(fd)), (i, fd, g[i])
