@@ -55,3 +55,13 @@ def test_pack_material_data_layout():
     assert pk.start[3] == lib[3].breaks.size and pk.coe_start[3] == lib[3].coefs.size
     assert pk.breaks.size == lib[3].breaks.size + lib[4].breaks.size
     assert np.array_equal(pk.coefs[:4], lib[3].coefs[0])
+
+
+def test_frequency_sweep_sizes_match_the_instances():
+    """The sizes the rank split is computed from are the instances' element counts."""
+    from magpackage_b200 import synth
+
+    sizes = synth.frequency_sweep_sizes(count=5, n_min=2, n_max=10)
+    got = [m.num_elements for m, *_ in synth.frequency_sweep_instances(count=5, n_min=2, n_max=10)]
+    assert sizes == got
+    assert len(synth.frequency_sweep_sizes()) == 64 and sum(synth.frequency_sweep_sizes()) == 12_848_640
