@@ -65,3 +65,23 @@ def test_frequency_sweep_sizes_match_the_instances():
     got = [m.num_elements for m, *_ in synth.frequency_sweep_instances(count=5, n_min=2, n_max=10)]
     assert sizes == got
     assert len(synth.frequency_sweep_sizes()) == 64 and sum(synth.frequency_sweep_sizes()) == 12_848_640
+
+
+@pytest.mark.parametrize("harmonics,n", [((0, 1, 3, 5), None), ((1, 3, 5), None), ((1, 7), 15), ((0, 2), 5)])
+def test_aft_round_trip_of_real_signals(harmonics, n):
+    """AFT (src/utils/AFT.m:19-86 restated): a real time signal x = Re(D X) made of the
+    listed harmonics goes back to X through P (a DC coefficient keeps its real part), and
+    the sample count follows the reference's rule."""
+    from magpackage_b200.hbfem import AFT
+
+    aft = AFT(harmonics, n)
+    h = np.asarray(harmonics)
+    want_n = max(32, 1 << int(np.ceil(np.log2(2 * h.max() + 1)))) if n is None else max(n, 2 * h.max() + 1)
+    assert aft.num_time_steps == want_n
+    assert aft.D.shape == (want_n, len(h)) and aft.P.shape == (len(h), want_n)
+    rng = np.random.default_rng(2)
+    X = rng.normal(size=len(h)) + 1j * rng.normal(size=len(h))
+    x = np.real(aft.D @ X)
+    back = aft.P @ x
+    want = np.where(h == 0, np.real(X), X)
+    np.testing.assert_allclose(back, want, rtol=0, atol=1e-12)
